@@ -1,0 +1,193 @@
+/*
+ * tigergrav_b200.h -- C ABI of the B200 periodic tree-gravity library
+ * (tigergrav_b200/libtigergrav_b200.so).
+ *
+ * The library replaces TigerGrav's gravity evaluation path: the tree built by
+ * tree::refine, the multipoles of tree::compute_multipoles, the dual-list walk
+ * of tree::kick_fmm with the eight gravity_{PP,PC,CC,CP}_{direct,ewald}
+ * kernels, L2L/L2P, and the kick/drift of the particle store.  All entry
+ * points are plain C: pointers, sizes, an int status, and a CUDA stream
+ * passed as `void *` (a cudaStream_t; NULL is the legacy default stream).
+ *
+ * Conventions
+ *  - Positions are the reference's int32 fixed point, x = i * 2^-32 + 0.5
+ *    (tigergrav/position.hpp:13-37), interleaved x,y,z per particle.
+ *  - Velocities and forces are interleaved x,y,z per particle.
+ *  - "where" arguments say whether a pointer is host (TG_HOST) or device
+ *    (TG_DEVICE) memory; host buffers are copied through pinned staging.
+ *  - Every call returns TG_OK (0) or a TG_ERR_* code; tg_error_string names it.
+ *  - A handle is not thread-safe; distinct handles may be used concurrently.
+ *  - Kernels never trap: bounded waits and capacity checks end in a status.
+ */
+#ifndef TIGERGRAV_B200_H
+#define TIGERGRAV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tg_status {
+    TG_OK = 0,
+    TG_ERR_ARG = 1,      /* bad argument (sizes, NULL pointers, NaN positions) */
+    TG_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+    TG_ERR_CAPACITY = 3, /* a list buffer overflowed and the retry limit was hit */
+    TG_ERR_DEPTH = 4,    /* more than leaf_max particles share a 63-level box */
+    TG_ERR_TIMEOUT = 5,  /* a bounded device wait ran out */
+    TG_ERR_STATE = 6,    /* call out of order (e.g. forces before a build) */
+    TG_ERR_NOMEM = 7     /* device allocation failed */
+};
+
+enum tg_precision {
+    TG_PREC_F32 = 0, /* FP32 interaction arithmetic, per-leaf compensated (Kahan) sums */
+    TG_PREC_F64 = 1  /* plain FP64 port: all interaction arithmetic in double */
+};
+
+enum tg_where { TG_HOST = 0, TG_DEVICE = 1 };
+
+/* Interaction-list kinds, CSR per node.  The first four are built at every
+ * node (tree.cpp:424-494), the last four at leaves (tree.cpp:530-629). */
+enum tg_list_kind {
+    TG_CC_D = 0, TG_CP_D = 1, TG_CC_E = 2, TG_CP_E = 3,
+    TG_PC_D = 4, TG_PP_D = 5, TG_PC_E = 6, TG_PP_E = 7
+};
+
+/* Solver parameters.  Replaces the reference's global options object
+ * (tigergrav/options.hpp:5-82) for the fields the gravity path reads. */
+typedef struct tg_params {
+    double theta;      /* opening angle; tree::set_theta (src/tree.cpp:93-111) */
+    double soft_len;   /* h, GADGET spline softening length (options::soft_len) */
+    double m;          /* particle mass, m_tot / problem_size (src/gravity.cpp:186) */
+    double G;          /* gravitational constant (options::G) */
+    int32_t ewald;     /* 1: periodic box with Ewald correction (options::ewald) */
+    int32_t leaf_max;  /* parts_per_node, 1..128 (src/options.cpp:52) */
+    int32_t precision; /* tg_precision */
+    int32_t device;    /* CUDA device ordinal */
+} tg_params;
+
+typedef struct tg_stats {
+    int64_t n;            /* particles */
+    int64_t nodes;        /* tree nodes (including empty ones) */
+    int64_t leaves;
+    int32_t depth;        /* deepest level */
+    int32_t walk_retries; /* list-buffer regrowths in the last walk */
+    /* interaction_stats as the reference files them (tigergrav/tree.hpp:84-114):
+     * PP_direct, PP_ewald, CC_direct, CC_ewald, CP_direct, CP_ewald
+     * (leaf PC counts filed under CP, as src/tree.cpp:618,627 do) */
+    uint64_t ref_stats[6];
+    /* per-kind interaction counts: PP_D, PP_E, PC_D, PC_E (sink-source pairs),
+     * CC_D, CC_E (node-node), CP_D, CP_E (node-particle) */
+    uint64_t counts[8];
+    double flops;         /* reference flop convention (src/gravity.cpp:299-784, tree.cpp:234) */
+    /* device time of the last solve, per phase, milliseconds */
+    double ms_build, ms_multipoles, ms_walk, ms_nodes, ms_leaves, ms_kick_drift;
+    int64_t launches;     /* kernels of this library launched on this handle so far */
+} tg_stats;
+
+typedef struct tg_solver tg_solver;
+
+const char *tg_error_string(int status);
+/* library version string */
+const char *tg_version(void);
+
+/* ---- solver object -------------------------------------------------- */
+/* Replaces options::process_options + tree::set_theta (src/options.cpp:28-94,
+ * src/tree.cpp:93-111): validates and stores the parameters. */
+int tg_create(const tg_params *params, tg_solver **out);
+int tg_destroy(tg_solver *s);
+
+/* Replaces part_vect_init (src/part_vect.cpp:654-673): loads n particles.
+ * x: n*3 int32, v: n*3 float (NULL = zero velocities). */
+int tg_set_particles(tg_solver *s, const int32_t *x, const float *v, int64_t n, int where, void *stream);
+/* Positions / velocities in the caller's original particle order. */
+int tg_get_particles(tg_solver *s, int32_t *x, float *v, int where, void *stream);
+
+/* tree::refine iterated to completion (src/tree.cpp:122-201, src/main.cpp:171-175). */
+int tg_build(tg_solver *s, void *stream);
+/* tree::compute_multipoles (src/tree.cpp:203-296). */
+int tg_multipoles(tg_solver *s, void *stream);
+/* tree::kick_fmm list generation (src/tree.cpp:378-635). */
+int tg_walk(tg_solver *s, void *stream);
+/* kick_fmm evaluation: CC/CP, L2L, L2P, PC/PP, direct and Ewald. */
+int tg_forces(tg_solver *s, void *stream);
+/* solve_gravity (src/main.cpp:31-73): build + multipoles + walk + forces. */
+int tg_solve_gravity(tg_solver *s, void *stream);
+
+/* Forces in the caller's order: phi[n], g[n*3] (either may be NULL). */
+int tg_get_forces(tg_solver *s, float *phi, float *g, int where, void *stream);
+int tg_get_forces_f64(tg_solver *s, double *phi, double *g, int where, void *stream);
+
+/* Kick with the last forces: v += g * G * dt (part_vect_kick, src/part_vect.cpp:341-436,
+ * as a plain fixed-dt half kick). */
+int tg_kick(tg_solver *s, double dt, void *stream);
+/* Drift x = wrap(x + v dt), requantised (part_vect_drift, src/part_vect.cpp:493-540). */
+int tg_drift(tg_solver *s, double dt, void *stream);
+/* FP64 reductions: out[0] = E_kin, out[1] = E_pot (0.5 m phi G), out[2..4] = sum v / n. */
+int tg_energy(tg_solver *s, double out[5], void *stream);
+/* n_steps kick-drift-kick leapfrog steps of dt (first call computes forces if needed). */
+int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream);
+
+int tg_get_stats(tg_solver *s, tg_stats *out);
+
+/* ---- introspection (parity tests) ----------------------------------- */
+int64_t tg_num_nodes(tg_solver *s);
+/* Node arrays in host memory, level order; any pointer may be NULL.
+ * boxid = 1 << level | Morton prefix (src/tree.cpp:159-160, src/range.cpp:134-168). */
+int tg_get_nodes(tg_solver *s, uint64_t *boxid, int32_t *level, int64_t *pbegin, int64_t *pend,
+                 int32_t *child0, int32_t *parent, int32_t *x, float *r, float *rmax, float *m);
+/* perm[i] = caller index of the particle at sorted position i. */
+int tg_get_perm(tg_solver *s, int64_t *perm);
+int64_t tg_list_size(tg_solver *s, int kind);
+/* CSR copy of list `kind`: offsets[num_nodes+1], ids[list_size] (host). */
+int tg_get_list(tg_solver *s, int kind, int64_t *offsets, int32_t *ids);
+
+/* ---- kernel-level seams (all pointers device memory) ------------------
+ * The eight reference kernels (tigergrav/gravity.hpp:39-46) evaluated over
+ * many sink groups at once.  Group k has sinks [sink_off[k], sink_off[k+1])
+ * and sources [src_off[k], src_off[k+1]).  f is nsinks x 4 doubles
+ * (phi, gx, gy, gz) and L is ngroups x 35 doubles; both accumulate with +=.
+ * Multipole sources: src_m (17 floats each), src_x (3 int32 each).
+ * CC/CP sinks: sink_x holds one position per group.
+ * Parameters (h, m, ewald) come from params.  flops (may be NULL) receives
+ * the reference's flop count (src/gravity.cpp:299,365,425,485,613,677,730,784). */
+int tg_gravity_PP_direct(const tg_params *params, int64_t ngroups, const int64_t *sink_off,
+                         const int32_t *sink_x, const int64_t *src_off, const int32_t *src_x,
+                         double *f, int do_phi, uint64_t *flops, void *stream);
+int tg_gravity_PP_ewald(const tg_params *params, int64_t ngroups, const int64_t *sink_off,
+                        const int32_t *sink_x, const int64_t *src_off, const int32_t *src_x,
+                        double *f, uint64_t *flops, void *stream);
+int tg_gravity_PC_direct(const tg_params *params, int64_t ngroups, const int64_t *sink_off,
+                         const int32_t *sink_x, const int64_t *src_off, const float *src_m,
+                         const int32_t *src_x, double *f, uint64_t *flops, void *stream);
+int tg_gravity_PC_ewald(const tg_params *params, int64_t ngroups, const int64_t *sink_off,
+                        const int32_t *sink_x, const int64_t *src_off, const float *src_m,
+                        const int32_t *src_x, double *f, uint64_t *flops, void *stream);
+int tg_gravity_CC_direct(const tg_params *params, int64_t ngroups, const int32_t *sink_x,
+                         const int64_t *src_off, const float *src_m, const int32_t *src_x,
+                         double *L, uint64_t *flops, void *stream);
+int tg_gravity_CC_ewald(const tg_params *params, int64_t ngroups, const int32_t *sink_x,
+                        const int64_t *src_off, const float *src_m, const int32_t *src_x,
+                        double *L, uint64_t *flops, void *stream);
+int tg_gravity_CP_direct(const tg_params *params, int64_t ngroups, const int32_t *sink_x,
+                         const int64_t *src_off, const int32_t *src_x, double *L,
+                         uint64_t *flops, void *stream);
+int tg_gravity_CP_ewald(const tg_params *params, int64_t ngroups, const int32_t *sink_x,
+                        const int64_t *src_off, const int32_t *src_x, double *L,
+                        uint64_t *flops, void *stream);
+
+/* ---- measurement ------------------------------------------------------
+ * FP64 direct Ewald sum (ground truth) at ns sample particles of the
+ * current particle set: phi[ns], g[ns*3] in host memory.  alpha is the
+ * Ewald split (>= 4.2); results are independent of it to ~1e-13. */
+int tg_truth(tg_solver *s, const int64_t *samples, int64_t ns, double alpha, double *phi, double *g,
+             void *stream);
+/* Measured FP32 FMA throughput of the device (TFLOP/s, 2 flops per FMA) from
+ * a register-resident FMA kernel: the denominator of the interaction
+ * kernels' roofline.  No counterpart in the reference. */
+int tg_device_fp32_peak(int device, double *tflops, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -274,7 +274,8 @@ class Oracle:
         assert lib().tgo_walk(self.h) == 0
         return self
 
-    def evaluate(self, use_ref=False, nthreads=0, leaf_subset=None):
+    def evaluate(self, use_ref=False, nthreads=0, leaf_subset=None, fp64=False):
+        """use_ref: the reference's own kernels; fp64: the restated kernels in double."""
         if use_ref:
             if ref_lib() is None:
                 raise RuntimeError("reference kernels not built (oracle/_ref)")
@@ -283,7 +284,8 @@ class Oracle:
                 raise RuntimeError("tgo_load_reference: %d" % rc)
         nt = nthreads or os.cpu_count() or 1
         sub = None if leaf_subset is None else np.ascontiguousarray(leaf_subset, np.int32)
-        rc = lib().tgo_evaluate(self.h, int(use_ref), nt, _p(sub), 0 if sub is None else len(sub))
+        mode = 1 if use_ref else (2 if fp64 else 0)
+        rc = lib().tgo_evaluate(self.h, mode, nt, _p(sub), 0 if sub is None else len(sub))
         if rc != 0:
             raise RuntimeError("tgo_evaluate: %d" % rc)
         return self

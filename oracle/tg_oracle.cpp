@@ -156,517 +156,120 @@ struct PeriodicParts {
 };
 const PeriodicParts PERIODIC;
 
-/* erfc by Abramowitz & Stegun 7.1.26 and exp(-x^2) (tigergrav/simd.hpp:676-692) */
-inline float erfcexp(float x, float *e) {
-    const float p = 0.3275911f, a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f,
-                a4 = -1.453152027f, a5 = 1.061405429f;
-    const float t1 = 1.0f / (1.0f + p * x);
-    const float t2 = t1 * t1;
-    const float t3 = t2 * t1;
-    const float t4 = t2 * t2;
-    const float t5 = t2 * t3;
-    *e = std::exp(-x * x);
-    return (a1 * t1 + a2 * t2 + a3 * t3 + a4 * t4 + a5 * t5) * *e;
-}
+template <class R> struct Fac;
+template <> struct Fac<float> {
+    static const Factors<float> &get() { return FF; }
+};
+template <> struct Fac<double> {
+    static const Factors<double> &get() { return FD; }
+};
 
-inline float fdot(const float *a, const float *b) {
-    float r = a[0] * b[0];
-    r += a[1] * b[1];
-    r += a[2] * b[2];
-    return r;
-}
-
-/* green_deriv_direct (tigergrav/green.hpp:62-117) */
-void green_deriv_direct(float *D, float d0, float d1, float d2, float d3, float d4, const float *dx) {
-    const float two = 2.0f;
-    D[E0()] = d0;
-    for (int a = 0; a < 3; a++) {
-        D[E1(a)] = dx[a] * d1;
-        for (int b = 0; b <= a; b++) {
-            const float dxadxb = dx[a] * dx[b];
-            D[E2(a, b)] = dxadxb * d2;
-            for (int c = 0; c <= b; c++) {
-                const float dxadxbdxc = dxadxb * dx[c];
-                D[E3(a, b, c)] = dxadxbdxc * d3;
-                for (int d = 0; d <= c; d++) {
-                    D[E4(a, b, c, d)] = dxadxbdxc * dx[d] * d4;
-                }
-            }
-        }
-    }
-    for (int a = 0; a < 3; a++) {
-        float &Daa = D[E2(a, a)];
-        float &Daaa = D[E3(a, a, a)];
-        float &Daaaa = D[E4(a, a, a, a)];
-        Daa += d1;
-        Daaa = std::fma(dx[a], d2, Daaa);
-        Daaaa = std::fma(dx[a] * dx[a], d3, Daaaa);
-        Daaaa = std::fma(two, d2, Daaaa);
-        for (int b = 0; b <= a; b++) {
-            float &Daab = D[E3(a, a, b)];
-            float &Dabb = D[E3(a, b, b)];
-            float &Daaab = D[E4(a, a, a, b)];
-            float &Daabb = D[E4(a, a, b, b)];
-            float &Dabbb = D[E4(a, b, b, b)];
-            const float dxadxb = dx[a] * dx[b];
-            Daab = std::fma(dx[b], d2, Daab);
-            Dabb = std::fma(dx[a], d2, Dabb);
-            Daaab = std::fma(dxadxb, d3, Daaab);
-            Dabbb = std::fma(dxadxb, d3, Dabbb);
-            Daabb += d2;
-            for (int c = 0; c <= b; c++) {
-                float &Daabc = D[E4(a, a, b, c)];
-                float &Dabcc = D[E4(a, b, c, c)];
-                float &Dabbc = D[E4(a, b, b, c)];
-                Daabc = std::fma(dx[b], dx[c] * d3, Daabc);
-                Dabcc = std::fma(dxadxb, d3, Dabcc);
-                Dabbc = std::fma(dx[a], dx[c] * d3, Dabbc);
-            }
-        }
-    }
-}
-
-/* green_deriv_ewald (tigergrav/green.hpp:119-165): float terms into double D */
-void green_deriv_ewald(double *D, float d0, float d1, float d2, float d3, float d4, const float *dx) {
-    const float two = 2.0f;
-    D[E0()] += d0;
-    for (int a = 0; a < 3; a++) {
-        D[E1(a)] += dx[a] * d1;
-        D[E2(a, a)] += d1;
-        D[E3(a, a, a)] += dx[a] * d2;
-        D[E4(a, a, a, a)] += dx[a] * dx[a] * d3;
-        D[E4(a, a, a, a)] += two * d2;
-        for (int b = 0; b <= a; b++) {
-            const float dxadxb = dx[a] * dx[b];
-            D[E2(a, b)] += dxadxb * d2;
-            D[E3(a, a, b)] += dx[b] * d2;
-            D[E3(a, b, b)] += dx[a] * d2;
-            D[E4(a, a, a, b)] += dxadxb * d3;
-            D[E4(a, b, b, b)] += dxadxb * d3;
-            D[E4(a, a, b, b)] += d2;
-            for (int c = 0; c <= b; c++) {
-                const float dxadxbdxc = dxadxb * dx[c];
-                D[E3(a, b, c)] += dxadxbdxc * d3;
-                D[E4(a, a, b, c)] += dx[b] * dx[c] * d3;
-                D[E4(a, b, c, c)] += dxadxb * d3;
-                D[E4(a, b, b, c)] += dx[a] * dx[c] * d3;
-                for (int d = 0; d <= c; d++) {
-                    D[E4(a, b, c, d)] += dxadxbdxc * dx[d] * d4;
-                }
-            }
-        }
-    }
-}
-
-/* green_direct (tigergrav/green.hpp:167-186) */
-void green_direct(const float *dX, float *D) {
-    const float r0 = 1.0e-9f;
-    const float r2 = fdot(dX, dX);
-    const float r = std::sqrt(r2);
-    const float rinv = (r > r0 ? 1.0f : 0.0f) / std::max(r, r0);
-    const float r2inv = rinv * rinv;
-    const float d0 = -rinv;
-    const float d1 = -d0 * r2inv;
-    const float d2 = -3.0f * d1 * r2inv;
-    const float d3 = -5.0f * d2 * r2inv;
-    const float d4 = -7.0f * d3 * r2inv;
-    green_deriv_direct(D, d0, d1, d2, d3, d4, dX);
-}
-
-/* green_ewald (tigergrav/green.hpp:189-286) */
-void green_ewald(const float *X, float *rcD) {
-    double D[LP];
-    for (int i = 0; i < LP; i++) D[i] = 0.0;
-    const float rcut = 1.0e-6f;
-    const float fouroversqrtpi = (float)(4.0 / std::sqrt(M_PI));
-    const float r0 = std::sqrt(fdot(X, X));
-    const float zmask = r0 > rcut ? 1.0f : 0.0f;
-    for (auto &nv : REAL_IDX.v) {
-        float dx[3] = {X[0] - nv[0], X[1] - nv[1], X[2] - nv[2]};
-        const float r2 = fdot(dx, dx);
-        const float r4 = r2 * r2;
-        const float r = std::sqrt(r2);
-        const float mask = (r < 3.6f ? 1.0f : 0.0f) * zmask;
-        const float rinv = mask / std::max(r, rcut);
-        const float r2inv = rinv * rinv;
-        const float r3inv = r2inv * rinv;
-        const float r5inv = r2inv * r3inv;
-        const float r7inv = r2inv * r5inv;
-        const float r9inv = r2inv * r7inv;
-        float expfac;
-        const float erfc = erfcexp(2.0f * r, &expfac);
-        const float expfactor = fouroversqrtpi * r * expfac;
-        const float d0 = -erfc * rinv;
-        const float d1 = (expfactor + erfc) * r3inv;
-        const float d2 = -std::fma(expfactor, std::fma(8.0f, r2, 3.0f), 3.0f * erfc) * r5inv;
-        const float d3 = std::fma(expfactor, (15.0f + std::fma(40.0f, r2, 64.0f * r4)), 15.0f * erfc) * r7inv;
-        const float d4 = -std::fma(expfactor, std::fma(8.0f * r2, (35.0f + std::fma(56.0f, r2, 64.0f * r4)), 105.0f),
-                                   105.0f * erfc) * r9inv;
-        green_deriv_ewald(D, d0, d1, d2, d3, d4, dx);
-    }
-    const float twopi = (float)(2.0 * M_PI);
-    for (size_t i = 0; i < FOUR_IDX.v.size(); i++) {
-        const auto &hv = FOUR_IDX.v[i];
-        const auto &H = PERIODIC.H[i];
-        float hdotdx = X[0] * hv[0];
-        hdotdx += X[1] * hv[1];
-        hdotdx += X[2] * hv[2];
-        const float omega = twopi * hdotdx;
-        float si = std::sin(omega) * zmask;
-        float co = std::cos(omega) * zmask;
-        D[E0()] += H[E0()] * co;
-        for (int a = 0; a < 3; a++) {
-            D[E1(a)] += H[E1(a)] * si;
-            for (int b = 0; b <= a; b++) {
-                D[E2(a, b)] += H[E2(a, b)] * co;
-                for (int c = 0; c <= b; c++) {
-                    D[E3(a, b, c)] += H[E3(a, b, c)] * si;
-                    for (int d = 0; d <= c; d++) {
-                        D[E4(a, b, c, d)] += H[E4(a, b, c, d)] * co;
+/* periodic_parts without the float rounding of c0, for the FP64 kernels */
+struct PeriodicPartsD {
+    std::vector<std::array<double, LP>> H;
+    PeriodicPartsD() {
+        for (auto &hv : FOUR_IDX.v) {
+            const double h[3] = {hv[0], hv[1], hv[2]};
+            const double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+            std::array<double, LP> D;
+            D.fill(0.0);
+            if (h2 > 0) {
+                const double c0 = 1.0 / h2 * std::exp(-M_PI * M_PI * h2 / 4.0);
+                D[E0()] = -(1.0 / M_PI) * c0;
+                for (int a = 0; a < 3; a++) {
+                    D[E1(a)] = 2.0 * h[a] * c0;
+                    for (int b = 0; b <= a; b++) {
+                        D[E2(a, b)] = 4.0 * M_PI * h[a] * h[b] * c0;
+                        for (int c = 0; c <= b; c++) {
+                            D[E3(a, b, c)] = -8.0 * M_PI * M_PI * h[a] * h[b] * h[c] * c0;
+                            for (int d = 0; d <= c; d++)
+                                D[E4(a, b, c, d)] = -16.0 * M_PI * M_PI * M_PI * h[a] * h[b] * h[c] * h[d] * c0;
+                        }
                     }
                 }
             }
+            H.push_back(D);
         }
     }
-    for (int i = 0; i < LP; i++) rcD[i] = (float)D[i];
-    float D1[LP];
-    green_direct(X, D1);
-    const float rinv = -zmask * D1[E0()];
-    rcD[E0()] = (float)(M_PI / 4.0) + rcD[E0()] + rinv;
-    rcD[E0()] = std::fma(2.8372975f, (1.0f - zmask), rcD[E0()] * zmask);
-    for (int a = 0; a < 3; a++) {
-        rcD[E1(a)] = zmask * (rcD[E1(a)] - D1[E1(a)]);
-        for (int b = 0; b <= a; b++) {
-            rcD[E2(a, b)] = zmask * (rcD[E2(a, b)] - D1[E2(a, b)]);
-            for (int c = 0; c <= b; c++) {
-                rcD[E3(a, b, c)] = zmask * (rcD[E3(a, b, c)] - D1[E3(a, b, c)]);
-                for (int d = 0; d <= c; d++) {
-                    rcD[E4(a, b, c, d)] = zmask * (rcD[E4(a, b, c, d)] - D1[E4(a, b, c, d)]);
-                }
-            }
-        }
-    }
+};
+const PeriodicPartsD PERIODIC_D;
+template <class R> struct Per;
+template <> struct Per<float> {
+    static const PeriodicParts &get() { return PERIODIC; }
+};
+template <> struct Per<double> {
+    static const PeriodicPartsD &get() { return PERIODIC_D; }
+};
+template <class R> inline void load_m(R *M, const float *ym) {
+    for (int k = 0; k < MP; k++) M[k] = (R)ym[k];
 }
 
-/* multipole -> expansion (M2L), src/gravity.cpp:26-90 */
-void mi_M2L(double *L, const float *M, const float *D) {
-    const auto &ef = FF.f;
-    double &L0 = L[E0()];
-    L0 += M[0] * D[E0()];
-    for (int a = 0; a < 3; a++) {
-        for (int b = a; b < 3; b++) {
-            L0 += M[M2i(a, b)] * D[E2(a, b)] * ef[E2(a, b)];
-            for (int c = b; c < 3; c++) {
-                L0 -= M[M3i(a, b, c)] * D[E3(a, b, c)] * ef[E3(a, b, c)];
-            }
-        }
-    }
-    for (int a = 0; a < 3; a++) {
-        double &La = L[E1(a)];
-        La += M[0] * D[E1(a)];
-        for (int b = 0; b < 3; b++) {
-            for (int c = b; c < 3; c++) {
-                La += M[M2i(c, b)] * D[E3(a, b, c)] * ef[E2(c, b)];
-                for (int d = c; d < 3; d++) {
-                    La -= M[M3i(b, c, d)] * D[E4(a, b, c, d)] * ef[E3(b, c, d)];
-                }
-            }
-        }
-    }
-    for (int a = 0; a < 3; a++) {
-        for (int b = a; b < 3; b++) {
-            double &Lab = L[E2(a, b)];
-            Lab += M[0] * D[E2(a, b)];
-            for (int c = 0; c < 3; c++) {
-                for (int d = c; d < 3; d++) {
-                    Lab += M[M2i(c, d)] * D[E4(a, b, c, d)] * ef[E2(c, d)];
-                }
-            }
-        }
-    }
-    for (int a = 0; a < 3; a++)
-        for (int b = a; b < 3; b++)
-            for (int c = b; c < 3; c++) {
-                L[E3(a, b, c)] += M[0] * D[E3(a, b, c)];
-            }
-    for (int a = 0; a < 3; a++)
-        for (int b = a; b < 3; b++)
-            for (int c = b; c < 3; c++)
-                for (int d = c; d < 3; d++) {
-                    L[E4(a, b, c, d)] += M[0] * D[E4(a, b, c, d)];
-                }
-}
-
-/* point mass -> expansion (P2L), src/gravity.cpp:92-121 */
-void mi_P2L(double *L, float M, const float *D) {
-    L[E0()] += M * D[E0()];
-    for (int a = 0; a < 3; a++) {
-        L[E1(a)] += M * D[E1(a)];
-        for (int b = a; b < 3; b++) {
-            L[E2(a, b)] += M * D[E2(a, b)];
-            for (int c = b; c < 3; c++) {
-                L[E3(a, b, c)] += M * D[E3(a, b, c)];
-                for (int d = c; d < 3; d++) {
-                    L[E4(a, b, c, d)] += M * D[E4(a, b, c, d)];
-                }
-            }
-        }
-    }
-}
-
-/* multipole -> particle (M2P), src/gravity.cpp:123-169.  The potential's
- * octupole sum runs a over all three axes (lines 141-147), as in the reference. */
-void mi_M2P(double *phi, double *g, const float *M, const float *D) {
-    const auto &ef = FF.f;
-    double ffirst = M[0] * D[E0()];
-    for (int a = 0; a < 3; a++)
-        for (int b = a; b < 3; b++) ffirst += M[M2i(a, b)] * D[E2(a, b)] * ef[E2(a, b)];
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = b; c < 3; c++) ffirst -= M[M3i(a, b, c)] * D[E3(a, b, c)] * ef[E3(a, b, c)];
-    double gs[3] = {0.0, 0.0, 0.0};
-    for (int a = 0; a < 3; a++) gs[a] -= M[0] * D[E1(a)];
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = b; c < 3; c++) gs[a] -= M[M2i(c, b)] * D[E3(a, b, c)] * ef[E2(c, b)];
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = b; c < 3; c++)
-                for (int d = c; d < 3; d++) gs[a] += M[M3i(c, b, d)] * D[E4(a, b, c, d)] * ef[E3(b, c, d)];
-    *phi += ffirst;
-    for (int a = 0; a < 3; a++) g[a] += gs[a];
-}
-
-/* dX between fixed-point positions (src/gravity.cpp:221-230) */
-inline void sep(const tgo_params *p, const int32_t *X, const int32_t *Y, float *dX, bool force_wrap) {
-    for (int d = 0; d < 3; d++) {
-        if (p->ewald || force_wrap) {
-            const int32_t diff = (int32_t)((uint32_t)X[d] - (uint32_t)Y[d]);
-            dX[d] = (float)((double)diff * POS_INV);
-        } else {
-            dX[d] = (float)((double)X[d] * POS_INV - (double)Y[d] * POS_INV);
-        }
-    }
-}
+/* The kernels in the reference's arithmetic (R = float) and in plain FP64
+ * (R = double, the double-precision oracle for the FP64 GPU path). */
+namespace k32 {
+using R = float;
+#include "tg_oracle_kernels.inc"
+} // namespace k32
+namespace k64 {
+using R = double;
+#include "tg_oracle_kernels.inc"
+} // namespace k64
 
 } // namespace
 
 extern "C" {
 
-/* gravity_PP_direct, src/gravity.cpp:171-300 */
 uint64_t tgo_PP_direct(const tgo_params *p, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi) {
-    if (nx == 0) return 0;
-    const double h = p->soft_len;
-    const float H = (float)h, halfH = (float)(0.5 * h), Hinv = (float)(1.0 / h), H3inv = (float)(1.0 / h / h / h);
-    const double phi_self = (-315.0 / 128.0) * p->m / h;
-    const float M = (float)p->m;
-    for (int i = 0; i < nx; i++) {
-        double G[3] = {0, 0, 0}, Phi = 0;
-        for (int j = 0; j < ny; j++) {
-            float dX[3];
-            sep(p, x + 3 * i, y + 3 * j, dX, false);
-            const float r2 = fdot(dX, dX);
-            const float r = std::sqrt(r2);
-            const float rinv = 1.0f / std::max(r, halfH);
-            const float rinv3 = rinv * rinv * rinv;
-            const float sw1 = r > H ? 1.0f : 0.0f;
-            const float sw3 = r < halfH ? 1.0f : 0.0f;
-            const float sw2 = 1.0f - sw1 - sw3;
-            const float roh = std::min(r * Hinv, 1.0f);
-            const float roh2 = roh * roh;
-            const float roh3 = roh2 * roh;
-            const float f1 = rinv3;
-            float f2 = (float)(-32.0 / 3.0);
-            f2 = std::fma(f2, roh, (float)(+192.0 / 5.0));
-            f2 = std::fma(f2, roh, -48.0f);
-            f2 = std::fma(f2, roh, (float)(+64.0 / 3.0));
-            f2 = std::fma(f2, roh3, (float)(-1.0 / 15.0));
-            f2 *= rinv3;
-            float f3 = 32.0f;
-            f3 = std::fma(f3, roh, (float)(-192.0 / 5.0));
-            f3 = std::fma(f3, roh2, (float)(+32.0 / 3.0));
-            f3 *= H3inv;
-            const float ff = sw1 * f1 + sw2 * f2 + sw3 * f3;
-            for (int d = 0; d < 3; d++) G[d] -= (double)((dX[d] * M) * ff);
-            if (do_phi) {
-                const float p1 = rinv;
-                float p2 = (float)(+32.0 / 15.0);
-                p2 = std::fma(p2, roh, (float)(-48.0 / 5.0));
-                p2 = std::fma(p2, roh, 16.0f);
-                p2 = std::fma(p2, roh, (float)(-32.0 / 3.0));
-                p2 = std::fma(p2, roh2, (float)(+16.0 / 5.0));
-                p2 = std::fma(p2, roh, (float)(-1.0 / 15.0));
-                p2 *= rinv;
-                float p3 = (float)(-32.0 / 5.0);
-                p3 = std::fma(p3, roh, (float)(+48.0 / 5.0));
-                p3 = std::fma(p3, roh2, (float)(-16.0 / 3.0));
-                p3 = std::fma(p3, roh2, (float)(+14.0 / 5.0));
-                p3 *= Hinv;
-                Phi -= (double)((sw1 * p1 + sw2 * p2 + sw3 * p3) * M);
-            }
-        }
-        f[4 * i + 1] += G[0];
-        f[4 * i + 2] += G[1];
-        f[4 * i + 3] += G[2];
-        f[4 * i + 0] += Phi;
-        f[4 * i + 0] -= phi_self;
-    }
-    return ((uint64_t)(74 + (do_phi ? 15 : 0)) * ny + 16 * 4 + 5) * nx;
+    return k32::k_PP_direct(p, f, x, nx, y, ny, do_phi);
 }
-
-/* gravity_PC_direct, src/gravity.cpp:302-366 */
 uint64_t tgo_PC_direct(const tgo_params *p, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny) {
-    if (nx == 0) return 0;
-    for (int i = 0; i < nx; i++) {
-        double Phi = 0, G[3] = {0, 0, 0};
-        for (int j = 0; j < ny; j++) {
-            float dX[3], D[LP];
-            sep(p, x + 3 * i, yx + 3 * j, dX, false);
-            green_direct(dX, D);
-            mi_M2P(&Phi, G, ym + MP * j, D);
-        }
-        for (int d = 0; d < 3; d++) f[4 * i + 1 + d] += G[d];
-        f[4 * i] += Phi;
-    }
-    return 581ull * ny * nx;
+    return k32::k_PC_direct(p, f, x, nx, ym, yx, ny);
 }
-
-/* gravity_CC_direct, src/gravity.cpp:368-426 */
 uint64_t tgo_CC_direct(const tgo_params *p, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny) {
-    if (ny == 0) return 0;
-    double Lacc[LP] = {0};
-    for (int j = 0; j < ny; j++) {
-        float dX[3], D[LP];
-        sep(p, x, yx + 3 * j, dX, false);
-        green_direct(dX, D);
-        mi_M2L(Lacc, ym + MP * j, D);
-    }
-    for (int i = 0; i < LP; i++) L[i] += Lacc[i];
-    return 1025ull * ny;
+    return k32::k_CC_direct(p, L, x, ym, yx, ny);
 }
-
-/* gravity_CP_direct, src/gravity.cpp:428-486 */
 uint64_t tgo_CP_direct(const tgo_params *p, double *L, const int32_t *x, const int32_t *y, int ny) {
-    if (ny == 0) return 0;
-    double Lacc[LP] = {0};
-    const float M = (float)p->m;
-    for (int j = 0; j < ny; j++) {
-        float dX[3], D[LP];
-        sep(p, x, y + 3 * j, dX, false);
-        green_direct(dX, D);
-        mi_P2L(Lacc, M, D);
-    }
-    for (int i = 0; i < LP; i++) L[i] += Lacc[i];
-    return 455ull * ny;
+    return k32::k_CP_direct(p, L, x, y, ny);
 }
-
-/* gravity_PP_ewald, src/gravity.cpp:491-614 (do_phi is ignored, as there) */
-uint64_t tgo_PP_ewald(const tgo_params *p, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int /*do_phi*/) {
-    if (nx == 0) return 0;
-    const double M = p->m;
-    const float rcut = 1.0e-6f;
-    const float twopi = (float)(2 * M_PI);
-    const float pioverfour = (float)(M_PI / 4.0);
-    const float fouroversqrtpi = (float)(4.0 / std::sqrt(M_PI));
-    const double phi0 = 2.8372975;
-    for (int I = 0; I < nx; I++) {
-        double Phi = 0, G[3] = {0, 0, 0};
-        for (int J = 0; J < ny; J++) {
-            float dX0[3];
-            sep(p, x + 3 * I, y + 3 * J, dX0, true);
-            double phi = 0.0, g[3] = {0, 0, 0};
-            const float r = std::sqrt(fdot(dX0, dX0));
-            const float cut_mask = r > rcut ? 1.0f : 0.0f;
-            for (auto &nv : REAL_IDX.v) {
-                const float dx[3] = {dX0[0] - nv[0], dX0[1] - nv[1], dX0[2] - nv[2]};
-                const float r2 = fdot(dx, dx);
-                const float rr = std::sqrt(r2);
-                const float mask = cut_mask * (rr < 3.6f ? 1.0f : 0.0f);
-                const float rinv = mask * 1.0f / std::max(rr, rcut);
-                const float r2inv = rinv * rinv;
-                const float r3inv = r2inv * rinv;
-                float expfac;
-                const float erfc = erfcexp(2.0f * rr, &expfac);
-                const float d0 = -erfc * rinv;
-                const float expfactor = fouroversqrtpi * rr * expfac;
-                const float d1 = (expfactor + erfc) * r3inv;
-                phi += d0;
-                for (int a = 0; a < 3; a++) g[a] -= (dX0[a] - nv[a]) * d1;
-            }
-            for (size_t i = 0; i < FOUR_IDX.v.size(); i++) {
-                const auto &H = PERIODIC.H[i];
-                const auto &hv = FOUR_IDX.v[i];
-                float hdotdx = dX0[0] * hv[0];
-                hdotdx += dX0[1] * hv[1];
-                hdotdx += dX0[2] * hv[2];
-                const float omega = twopi * hdotdx;
-                const float s = std::sin(omega), c = std::cos(omega);
-                phi += H[E0()] * c * cut_mask;
-                for (int d = 0; d < 3; d++) g[d] -= H[E1(d)] * s * cut_mask;
-            }
-            const float rinv = 1.0f / std::max(r, rcut);
-            phi += pioverfour + rinv;
-            const double sw = cut_mask;
-            phi = phi0 * (1.0 - sw) + phi * sw;
-            const float rinv3 = cut_mask * rinv * rinv * rinv;
-            for (int d = 0; d < 3; d++) g[d] += dX0[d] * rinv3;
-            Phi += M * phi;
-            for (int d = 0; d < 3; d++) G[d] += g[d] * M;
-        }
-        for (int d = 0; d < 3; d++) f[4 * I + 1 + d] += G[d];
-        f[4 * I] += Phi;
-    }
-    return 56245ull * ny * nx;
+uint64_t tgo_PP_ewald(const tgo_params *p, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi) {
+    return k32::k_PP_ewald(p, f, x, nx, y, ny, do_phi);
 }
-
-/* gravity_PC_ewald, src/gravity.cpp:616-678 */
 uint64_t tgo_PC_ewald(const tgo_params *p, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny) {
-    if (nx == 0) return 0;
-    for (int i = 0; i < nx; i++) {
-        double Phi = 0, G[3] = {0, 0, 0};
-        for (int j = 0; j < ny; j++) {
-            float dX[3], D[LP];
-            sep(p, x + 3 * i, yx + 3 * j, dX, true);
-            green_ewald(dX, D);
-            mi_M2P(&Phi, G, ym + MP * j, D);
-        }
-        for (int d = 0; d < 3; d++) f[4 * i + 1 + d] += G[d];
-        f[4 * i] += Phi;
-    }
-    return 251531ull * ny * nx;
+    return k32::k_PC_ewald(p, f, x, nx, ym, yx, ny);
 }
-
-/* gravity_CC_ewald, src/gravity.cpp:680-731 */
 uint64_t tgo_CC_ewald(const tgo_params *p, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny) {
-    if (ny == 0) return 0;
-    double Lacc[LP] = {0};
-    for (int j = 0; j < ny; j++) {
-        float dX[3], D[LP];
-        sep(p, x, yx + 3 * j, dX, true);
-        green_ewald(dX, D);
-        mi_M2L(Lacc, ym + MP * j, D);
-    }
-    for (int i = 0; i < LP; i++) L[i] += Lacc[i];
-    return 251975ull * ny;
+    return k32::k_CC_ewald(p, L, x, ym, yx, ny);
 }
-
-/* gravity_CP_ewald, src/gravity.cpp:733-785 */
 uint64_t tgo_CP_ewald(const tgo_params *p, double *L, const int32_t *x, const int32_t *y, int ny) {
-    if (ny == 0) return 0;
-    double Lacc[LP] = {0};
-    const float M = (float)p->m;
-    for (int j = 0; j < ny; j++) {
-        float dX[3], D[LP];
-        sep(p, x, y + 3 * j, dX, true);
-        green_ewald(dX, D);
-        mi_P2L(Lacc, M, D);
-    }
-    for (int i = 0; i < LP; i++) L[i] += Lacc[i];
-    return 251233ull * ny;
+    return k32::k_CP_ewald(p, L, x, y, ny);
+}
+uint64_t tgo64_PP_direct(const tgo_params *p, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi) {
+    return k64::k_PP_direct(p, f, x, nx, y, ny, do_phi);
+}
+uint64_t tgo64_PC_direct(const tgo_params *p, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny) {
+    return k64::k_PC_direct(p, f, x, nx, ym, yx, ny);
+}
+uint64_t tgo64_CC_direct(const tgo_params *p, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny) {
+    return k64::k_CC_direct(p, L, x, ym, yx, ny);
+}
+uint64_t tgo64_CP_direct(const tgo_params *p, double *L, const int32_t *x, const int32_t *y, int ny) {
+    return k64::k_CP_direct(p, L, x, y, ny);
+}
+uint64_t tgo64_PP_ewald(const tgo_params *p, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi) {
+    return k64::k_PP_ewald(p, f, x, nx, y, ny, do_phi);
+}
+uint64_t tgo64_PC_ewald(const tgo_params *p, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny) {
+    return k64::k_PC_ewald(p, f, x, nx, ym, yx, ny);
+}
+uint64_t tgo64_CC_ewald(const tgo_params *p, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny) {
+    return k64::k_CC_ewald(p, L, x, ym, yx, ny);
+}
+uint64_t tgo64_CP_ewald(const tgo_params *p, double *L, const int32_t *x, const int32_t *y, int ny) {
+    return k64::k_CP_ewald(p, L, x, y, ny);
 }
 
-void tgo_green_ewald(const float dx[3], float D[35]) { green_ewald(dx, D); }
-void tgo_green_direct(const float dx[3], float D[35]) { green_direct(dx, D); }
+void tgo_green_ewald(const float dx[3], float D[35]) { k32::green_ewald(dx, D); }
+void tgo_green_direct(const float dx[3], float D[35]) { k32::green_direct(dx, D); }
 
 /* expansion<double>::operator<<= (tigergrav/expansion.hpp:184-233) */
 void tgo_L2L(double *me, const double *dX) {
@@ -798,6 +401,7 @@ struct Solver {
     uint64_t ref_stats[6] = {0};
     uint64_t counts[8] = {0};
     std::atomic<uint64_t> flops{0};
+    uint64_t p2m_flops = 0; /* compute_multipoles share, src/tree.cpp:234 */
     double theta_inv = 0;
     float r_ewald = 0;
     /* reference kernel table */
@@ -965,6 +569,7 @@ int tgo_build(void *h) {
 int tgo_multipoles(void *h) {
     Solver &S = *(Solver *)h;
     const float mass = (float)S.p.m;
+    S.p2m_flops = 0;
     for (int64_t i = (int64_t)S.nodes.size() - 1; i >= 0; i--) {
         Node &nd = S.nodes[i];
         const int64_t cnt = nd.pe - nd.pb;
@@ -1039,7 +644,7 @@ int tgo_multipoles(void *h) {
                 nd.prmin[d] = nd.amin[d];
                 nd.prmax[d] = nd.amax[d];
             }
-            S.flops += (uint64_t)cnt * 64;
+            S.p2m_flops += (uint64_t)cnt * 64;
         } else {
             const Node &ml = S.nodes[nd.child0];
             const Node &mr = S.nodes[nd.child0 + 1];
@@ -1354,15 +959,22 @@ int tgo_load_reference(void *h, const char *so_path) {
  * PC_ewald, PP_ewald (src/tree.cpp:603-629). */
 int tgo_evaluate(void *h, int use_ref, int nthreads, const int32_t *leaf_subset, int64_t nsubset) {
     Solver &S = *(Solver *)h;
-    if (use_ref && !S.dl) return -1;
-    tgo_pp_fn pp_d = use_ref ? S.ref_pp_d : tgo_PP_direct, pp_e = use_ref ? S.ref_pp_e : tgo_PP_ewald;
-    tgo_pc_fn pc_d = use_ref ? S.ref_pc_d : tgo_PC_direct, pc_e = use_ref ? S.ref_pc_e : tgo_PC_ewald;
-    tgo_cc_fn cc_d = use_ref ? S.ref_cc_d : tgo_CC_direct, cc_e = use_ref ? S.ref_cc_e : tgo_CC_ewald;
-    tgo_cp_fn cp_d = use_ref ? S.ref_cp_d : tgo_CP_direct, cp_e = use_ref ? S.ref_cp_e : tgo_CP_ewald;
+    if (use_ref == 1 && !S.dl) return -1;
+    tgo_pp_fn pp_d = tgo_PP_direct, pp_e = tgo_PP_ewald;
+    tgo_pc_fn pc_d = tgo_PC_direct, pc_e = tgo_PC_ewald;
+    tgo_cc_fn cc_d = tgo_CC_direct, cc_e = tgo_CC_ewald;
+    tgo_cp_fn cp_d = tgo_CP_direct, cp_e = tgo_CP_ewald;
+    if (use_ref == 1) {
+        pp_d = S.ref_pp_d; pp_e = S.ref_pp_e; pc_d = S.ref_pc_d; pc_e = S.ref_pc_e;
+        cc_d = S.ref_cc_d; cc_e = S.ref_cc_e; cp_d = S.ref_cp_d; cp_e = S.ref_cp_e;
+    } else if (use_ref == 2) {
+        pp_d = tgo64_PP_direct; pp_e = tgo64_PP_ewald; pc_d = tgo64_PC_direct; pc_e = tgo64_PC_ewald;
+        cc_d = tgo64_CC_direct; cc_e = tgo64_CC_ewald; cp_d = tgo64_CP_direct; cp_e = tgo64_CP_ewald;
+    }
     const size_t nn = S.nodes.size();
     S.L.assign(nn * LP, 0.0);
     S.f.assign(S.n * 4, 0.0);
-    S.flops = 0;
+    S.flops = S.p2m_flops;
     std::vector<char> active(nn, leaf_subset ? 0 : 1);
     std::vector<int32_t> leaves;
     if (leaf_subset) {

@@ -60,6 +60,16 @@ uint64_t tgo_PC_ewald(const tgo_params *, double *f, const int32_t *x, int nx, c
 uint64_t tgo_CC_ewald(const tgo_params *, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny);
 uint64_t tgo_CP_ewald(const tgo_params *, double *L, const int32_t *x, const int32_t *y, int ny);
 
+/* the same kernels with every interaction computed in double (FP64 oracle) */
+uint64_t tgo64_PP_direct(const tgo_params *, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi);
+uint64_t tgo64_PC_direct(const tgo_params *, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny);
+uint64_t tgo64_CC_direct(const tgo_params *, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny);
+uint64_t tgo64_CP_direct(const tgo_params *, double *L, const int32_t *x, const int32_t *y, int ny);
+uint64_t tgo64_PP_ewald(const tgo_params *, double *f, const int32_t *x, int nx, const int32_t *y, int ny, int do_phi);
+uint64_t tgo64_PC_ewald(const tgo_params *, double *f, const int32_t *x, int nx, const float *ym, const int32_t *yx, int ny);
+uint64_t tgo64_CC_ewald(const tgo_params *, double *L, const int32_t *x, const float *ym, const int32_t *yx, int ny);
+uint64_t tgo64_CP_ewald(const tgo_params *, double *L, const int32_t *x, const int32_t *y, int ny);
+
 /* green_ewald(dX) in the reference's FP32 arithmetic (tigergrav/green.hpp:189-286): D[35] */
 void tgo_green_ewald(const float dx[3], float D[35]);
 /* green_direct(dX) (tigergrav/green.hpp:167-186): D[35] */
@@ -81,8 +91,9 @@ int tgo_build(void *h);
 int tgo_multipoles(void *h);
 /* kick_fmm list generation (src/tree.cpp:378-635) */
 int tgo_walk(void *h);
-/* Evaluate forces along the lists. use_ref: 0 = restated kernels, 1 = the
- * reference's kernels loaded by tgo_load_reference.  nthreads >= 1.
+/* Evaluate forces along the lists. use_ref: 0 = restated kernels (reference
+ * arithmetic), 1 = the reference's kernels loaded by tgo_load_reference,
+ * 2 = restated kernels in FP64.  nthreads >= 1.
  * leaf_subset (may be NULL): evaluate only these leaves (node ids) and the
  * nodes on their root paths; forces of other particles are left at zero.   */
 int tgo_evaluate(void *h, int use_ref, int nthreads, const int32_t *leaf_subset, int64_t nsubset);

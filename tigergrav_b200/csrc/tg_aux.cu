@@ -1,0 +1,495 @@
+/*
+ * tg_aux.cu -- constants, Ewald tables, kick/drift, reductions, particle
+ * packing, and the FP64 direct Ewald-sum ground truth.
+ */
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <vector>
+
+#include "tg_solver.cuh"
+
+namespace tg {
+
+/* expansion_factors (tigergrav/expansion.hpp:162-182) accumulated in T */
+template <class T>
+static void host_factors(T *f) {
+    for (int i = 0; i < LP; i++) f[i] = T(0);
+    f[E0()] += T(1);
+    for (int a = 0; a < 3; ++a) {
+        f[E1(a)] += T(1.0);
+        for (int b = 0; b < 3; ++b) {
+            f[E2(a, b)] += T(0.5);
+            for (int c = 0; c < 3; ++c) {
+                f[E3(a, b, c)] += T(1.0 / 6.0);
+                for (int d = 0; d < 3; ++d) f[E4(a, b, c, d)] += T(1.0 / 24.0);
+            }
+        }
+    }
+}
+
+int init_constants() {
+    float ff[LP];
+    double fd[LP];
+    host_factors(ff);
+    host_factors(fd);
+    TG_CUDA(cudaMemcpyToSymbol(c_factor_f, ff, sizeof(ff)));
+    TG_CUDA(cudaMemcpyToSymbol(c_factor_d, fd, sizeof(fd)));
+    return TG_OK;
+}
+
+/* ewald_indices (tigergrav/green.hpp:8-28): integer vectors with |v|^2 <= n2max,
+ * ordered by decreasing |v|^2 */
+static std::vector<std::array<int, 3>> lattice(int n2max) {
+    std::vector<std::array<int, 3>> v;
+    const int nmax = (int)std::sqrt((double)n2max) + 1;
+    for (int i = -nmax; i <= nmax; i++)
+        for (int j = -nmax; j <= nmax; j++)
+            for (int k = -nmax; k <= nmax; k++)
+                if (i * i + j * j + k * k <= n2max) v.push_back({i, j, k});
+    std::stable_sort(v.begin(), v.end(), [](const std::array<int, 3> &a, const std::array<int, 3> &b) {
+        return a[0] * a[0] + a[1] * a[1] + a[2] * a[2] > b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+    });
+    return v;
+}
+
+/* periodic_parts (tigergrav/green.hpp:30-59) in FP64: one thread per h */
+__global__ void k_periodic_parts(const float4 *four, int nf, double *Hd, float *Hf) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nf) return;
+    const float4 hv = four[t];
+    const double h[3] = {hv.x, hv.y, hv.z};
+    const double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+    double D[LP];
+    float F[LP];
+    for (int i = 0; i < LP; i++) {
+        D[i] = 0.0;
+        F[i] = 0.0f;
+    }
+    if (h2 > 0) {
+        const double pi = 3.141592653589793;
+        const double c0 = 1.0 / h2 * exp(-pi * pi * h2 / 4.0);
+        const double c0f = (double)(float)c0; /* the reference stores c0 as float */
+        for (int pass = 0; pass < 2; pass++) {
+            const double c = pass ? c0f : c0;
+            double out[LP];
+            out[E0()] = -(1.0 / pi) * c;
+            for (int a = 0; a < 3; a++) {
+                out[E1(a)] = 2.0 * h[a] * c;
+                for (int b = 0; b <= a; b++) {
+                    out[E2(a, b)] = 4.0 * pi * h[a] * h[b] * c;
+                    for (int cc = 0; cc <= b; cc++) {
+                        out[E3(a, b, cc)] = -8.0 * pi * pi * h[a] * h[b] * h[cc] * c;
+                        for (int d = 0; d <= cc; d++)
+                            out[E4(a, b, cc, d)] = -16.0 * pi * pi * pi * h[a] * h[b] * h[cc] * h[d] * c;
+                    }
+                }
+            }
+            for (int i = 0; i < LP; i++) {
+                if (pass) F[i] = (float)out[i];
+                else D[i] = out[i];
+            }
+        }
+    }
+    for (int i = 0; i < LP; i++) {
+        Hd[LP * t + i] = D[i];
+        Hf[LP * t + i] = F[i];
+    }
+}
+
+int ewald_tables(Solver &S, cudaStream_t st) {
+    if (S.have_tables) return TG_OK;
+    const auto real = lattice(17), four = lattice(9);
+    if ((int)real.size() != NREAL || (int)four.size() != NFOUR) return TG_ERR_STATE;
+    std::vector<float4> r4(NREAL), f4(NFOUR);
+    for (int i = 0; i < NREAL; i++) r4[i] = make_float4((float)real[i][0], (float)real[i][1], (float)real[i][2], 0.0f);
+    for (int i = 0; i < NFOUR; i++) f4[i] = make_float4((float)four[i][0], (float)four[i][1], (float)four[i][2], 0.0f);
+    TG_TRY(ensure(S.ew_real, NREAL));
+    TG_TRY(ensure(S.ew_four, NFOUR));
+    TG_TRY(ensure(S.ew_Hf, NFOUR * LP));
+    TG_TRY(ensure(S.ew_Hd, NFOUR * LP));
+    TG_CUDA(cudaMemcpyAsync(S.ew_real.p, r4.data(), sizeof(float4) * NREAL, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(S.ew_four.p, f4.data(), sizeof(float4) * NFOUR, cudaMemcpyHostToDevice, st));
+    k_periodic_parts<<<(NFOUR + 63) / 64, 64, 0, st>>>(S.ew_four.p, NFOUR, S.ew_Hd.p, S.ew_Hf.p);
+    TG_TRY(launched(S));
+    TG_CUDA(cudaStreamSynchronize(st)); /* host vectors go out of scope */
+    S.have_tables = true;
+    return TG_OK;
+}
+
+/* ---- kick / drift ---- */
+
+/* v = v + float(g * (dt * G))  (src/part_vect.cpp:364,378) */
+__global__ void k_kick(int64_t n, float4 *vel, const float4 *acc, const double *accd, double dtG) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = vel[i];
+    double g[3];
+    if (accd) {
+        for (int d = 0; d < 3; d++) g[d] = accd[4 * i + 1 + d];
+    } else {
+        const float4 a = acc[i];
+        g[0] = a.y;
+        g[1] = a.z;
+        g[2] = a.w;
+    }
+    v.x = __fadd_rn(v.x, __double2float_rn(__dmul_rn(g[0], dtG)));
+    v.y = __fadd_rn(v.y, __double2float_rn(__dmul_rn(g[1], dtG)));
+    v.z = __fadd_rn(v.z, __double2float_rn(__dmul_rn(g[2], dtG)));
+    vel[i] = v;
+}
+
+/* x = wrap(x + v * dt), requantised (src/part_vect.cpp:513-530) */
+__global__ void k_drift(int64_t n, int4 *pos, const float4 *vel, float dt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int4 p = pos[i];
+    const float4 v = vel[i];
+    int *pp[3] = {&p.x, &p.y, &p.z};
+    const float vv[3] = {v.x, v.y, v.z};
+    for (int d = 0; d < 3; d++) {
+        double x = __dadd_rn(pos2d(*pp[d]), (double)__fmul_rn(vv[d], dt));
+        for (int it = 0; it < 4 && x >= 1.0; it++) x = __dadd_rn(x, -1.0);
+        for (int it = 0; it < 4 && x < 0.0; it++) x = __dadd_rn(x, 1.0);
+        *pp[d] = d2pos(x);
+    }
+    pos[i] = p;
+}
+
+int kick(Solver &S, double dt, cudaStream_t st) {
+    if (!S.have_forces) return TG_ERR_STATE;
+    const int64_t n = S.n;
+    const bool f64 = S.prm.precision == TG_PREC_F64;
+    k_kick<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.vel.p, f64 ? nullptr : S.acc.p, f64 ? S.accd.p : nullptr,
+                                                   dt * S.prm.G);
+    TG_TRY(launched(S));
+    return TG_OK;
+}
+
+int drift(Solver &S, double dt, cudaStream_t st) {
+    const int64_t n = S.n;
+    if (n <= 0) return TG_ERR_STATE;
+    k_drift<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.pos.p, S.vel.p, (float)dt);
+    TG_TRY(launched(S));
+    S.have_tree = S.have_multipoles = S.have_lists = S.have_forces = false;
+    return TG_OK;
+}
+
+/* ---- FP64 reductions (deterministic: fixed block partials, then one block) ---- */
+constexpr int RED_BLOCKS = 1024;
+
+__global__ void k_energy_partial(int64_t n, const float4 *vel, const float4 *acc, const double *accd, double m,
+                                 double G, double *part) {
+    __shared__ double sh[5][256];
+    double e[5] = {0, 0, 0, 0, 0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = vel[i];
+        const double vx = v.x, vy = v.y, vz = v.z;
+        e[0] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        const double phi = accd ? accd[4 * i] : (acc ? (double)acc[i].x : 0.0);
+        e[1] += 0.5 * m * phi * G;
+        e[2] += vx;
+        e[3] += vy;
+        e[4] += vz;
+    }
+    for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = e[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int k = 0; k < 5; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) part[5 * blockIdx.x + k] = sh[k][0];
+}
+
+__global__ void k_energy_final(int nb, const double *part, double *out) {
+    __shared__ double sh[5][256];
+    double e[5] = {0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+        for (int k = 0; k < 5; k++) e[k] += part[5 * b + k];
+    for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = e[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int k = 0; k < 5; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) out[k] = sh[k][0];
+}
+
+int energy(Solver &S, double out[5], cudaStream_t st) {
+    const int64_t n = S.n;
+    if (n <= 0) return TG_ERR_STATE;
+    DevBuf<double> part;
+    TG_TRY(ensure(part, 5 * RED_BLOCKS + 8));
+    const bool f64 = S.prm.precision == TG_PREC_F64;
+    const float4 *acc = (!f64 && S.have_forces) ? S.acc.p : nullptr;
+    const double *accd = (f64 && S.have_forces) ? S.accd.p : nullptr;
+    k_energy_partial<<<RED_BLOCKS, 256, 0, st>>>(n, S.vel.p, acc, accd, S.prm.m, S.prm.G, part.p);
+    k_energy_final<<<1, 256, 0, st>>>(RED_BLOCKS, part.p, part.p + 5 * RED_BLOCKS);
+    TG_TRY(launched(S));
+    S.launches++;
+    double h[5];
+    TG_CUDA(cudaMemcpyAsync(h, part.p + 5 * RED_BLOCKS, sizeof(h), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    release(part);
+    out[0] = h[0];
+    out[1] = h[1];
+    for (int d = 0; d < 3; d++) out[2 + d] = h[2 + d] / (double)n;
+    return TG_OK;
+}
+
+/* ---- FP64 direct Ewald sum (ground truth) ----
+ * psi(x) = -sum_n erfc(a|x-n|)/|x-n| - sum_{h!=0} exp(-pi^2 h^2/a^2)/(pi h^2) cos(2 pi h.x) + pi/a^2,
+ * the reference's periodic Green's function (tigergrav/green.hpp:30-59,189-286)
+ * for any split a.  Real-space images with a|x-n| < 6.2, reciprocal vectors
+ * with pi^2 h^2 / a^2 < 38; the reciprocal sum goes through structure factors
+ * S(h) = sum_j exp(2 pi i h.x_j).  Nearest-image pairs closer than h use the
+ * GADGET spline (src/gravity.cpp:231-287). */
+
+__global__ void k_sfac(int64_t n, const int4 *pos, int nh, const int4 *hv, double *part, int64_t chunk) {
+    /* block (hb, pc): threads = h vectors of this block, loop over particle chunk pc */
+    __shared__ double sx[256][3];
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.y * chunk, p1 = min(n, p0 + chunk);
+    int4 H = make_int4(0, 0, 0, 0);
+    if (h < nh) H = hv[h];
+    double c = 0.0, s = 0.0;
+    for (int64_t base = p0; base < p1; base += 256) {
+        __syncthreads();
+        const int64_t j = base + threadIdx.x;
+        if (threadIdx.x < 256 && j < p1) {
+            const int4 p = pos[j];
+            sx[threadIdx.x][0] = pos2d(p.x);
+            sx[threadIdx.x][1] = pos2d(p.y);
+            sx[threadIdx.x][2] = pos2d(p.z);
+        }
+        __syncthreads();
+        const int cnt = (int)min((int64_t)256, p1 - base);
+        if (h < nh) {
+            for (int q = 0; q < cnt; q++) {
+                const double arg = 2.0 * (H.x * sx[q][0] + H.y * sx[q][1] + H.z * sx[q][2]);
+                double sn, cs;
+                sincospi(arg, &sn, &cs);
+                c += cs;
+                s += sn;
+            }
+        }
+    }
+    if (h < nh) {
+        part[2 * ((int64_t)blockIdx.y * nh + h)] = c;
+        part[2 * ((int64_t)blockIdx.y * nh + h) + 1] = s;
+    }
+}
+
+__global__ void k_sfac_reduce(int nh, int nchunks, const double *part, double *S) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    double c = 0.0, s = 0.0;
+    for (int k = 0; k < nchunks; k++) {
+        c += part[2 * ((int64_t)k * nh + h)];
+        s += part[2 * ((int64_t)k * nh + h) + 1];
+    }
+    S[2 * h] = c;
+    S[2 * h + 1] = s;
+}
+
+/* one block per sample: real-space sum over all particles and images */
+__global__ void k_truth_real(int64_t n, const int4 *pos, const int64_t *sample_sorted, int64_t ns, double m, double h,
+                             double alpha, double *out) {
+    __shared__ double sh[4][256];
+    const int64_t k = blockIdx.x;
+    if (k >= ns) return;
+    const int4 xi = pos[sample_sorted[k]];
+    const double rcut = 6.2 / alpha;
+    const double two_a_sqrtpi = 2.0 * alpha / 1.7724538509055160273;
+    double phi = 0.0, g[3] = {0.0, 0.0, 0.0};
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const int4 y = pos[j];
+        const double d[3] = {wrap_sep_d(xi.x, y.x), wrap_sep_d(xi.y, y.y), wrap_sep_d(xi.z, y.z)};
+        for (int nx = -1; nx <= 1; nx++)
+            for (int ny = -1; ny <= 1; ny++)
+                for (int nz = -1; nz <= 1; nz++) {
+                    const double e[3] = {d[0] - nx, d[1] - ny, d[2] - nz};
+                    const double r2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+                    const double r = sqrt(r2);
+                    if (r >= rcut) continue;
+                    const bool nearest = (nx == 0 && ny == 0 && nz == 0);
+                    if (r == 0.0) {
+                        phi += m * two_a_sqrtpi + m * (-(14.0 / 5.0) / h + (315.0 / 128.0) / h);
+                        continue;
+                    }
+                    const double erfcv = erfc(alpha * r);
+                    const double ef = two_a_sqrtpi * r * exp(-alpha * alpha * r2);
+                    phi -= m * erfcv / r;
+                    double d1 = (ef + erfcv) / (r2 * r);
+                    if (nearest && r < h) {
+                        const double u = r / h;
+                        double fk, pk;
+                        if (u < 0.5) {
+                            fk = (32.0 * u * u * u - 192.0 / 5.0 * u * u + 32.0 / 3.0) / (h * h * h);
+                            pk = (-32.0 / 5.0 * u * u * u * u * u + 48.0 / 5.0 * u * u * u * u - 16.0 / 3.0 * u * u + 14.0 / 5.0) / h;
+                        } else {
+                            fk = (-32.0 / 3.0 * u * u * u + 192.0 / 5.0 * u * u - 48.0 * u + 64.0 / 3.0) / (h * h * h) -
+                                 1.0 / (15.0 * r2 * r);
+                            pk = (32.0 / 15.0 * u * u * u * u * u - 48.0 / 5.0 * u * u * u * u + 16.0 * u * u * u -
+                                  32.0 / 3.0 * u * u + 16.0 / 5.0) / h - 1.0 / (15.0 * r);
+                        }
+                        d1 += fk - 1.0 / (r2 * r);
+                        phi += m * (1.0 / r - pk);
+                    }
+                    for (int a = 0; a < 3; a++) g[a] -= m * e[a] * d1;
+                }
+    }
+    sh[0][threadIdx.x] = phi;
+    sh[1][threadIdx.x] = g[0];
+    sh[2][threadIdx.x] = g[1];
+    sh[3][threadIdx.x] = g[2];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 4; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; q++) out[4 * k + q] = sh[q][0];
+}
+
+/* reciprocal part at the samples */
+__global__ void k_truth_four(int64_t n, const int4 *pos, const int64_t *sample_sorted, int64_t ns, double m,
+                             double alpha, int nh, const int4 *hv, const double *S, double *out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    const int4 xi = pos[sample_sorted[k]];
+    const double x[3] = {pos2d(xi.x), pos2d(xi.y), pos2d(xi.z)};
+    const double pi = 3.141592653589793;
+    double phi = 0.0, g[3] = {0, 0, 0};
+    for (int q = 0; q < nh; q++) {
+        const int4 H = hv[q];
+        const double hh = (double)(H.x * H.x + H.y * H.y + H.z * H.z);
+        const double c0 = exp(-pi * pi * hh / (alpha * alpha)) / hh;
+        double si, ci;
+        sincospi(2.0 * (H.x * x[0] + H.y * x[1] + H.z * x[2]), &si, &ci);
+        const double sc = ci * S[2 * q] + si * S[2 * q + 1];
+        const double ss = si * S[2 * q] - ci * S[2 * q + 1];
+        phi += 2.0 * m * (-(1.0 / pi) * c0 * sc);
+        g[0] -= 4.0 * m * H.x * c0 * ss;
+        g[1] -= 4.0 * m * H.y * c0 * ss;
+        g[2] -= 4.0 * m * H.z * c0 * ss;
+    }
+    phi += m * (double)n * pi / (alpha * alpha);
+    out[4 * k] += phi;
+    for (int a = 0; a < 3; a++) out[4 * k + 1 + a] += g[a];
+}
+
+__global__ void k_find_sorted(int64_t n, const int4 *pos, int64_t *caller_to_sorted) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    caller_to_sorted[pos[i].w] = i;
+}
+
+__global__ void k_pick(const int64_t *map, const int64_t *samples, int64_t ns, int64_t *out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    out[k] = map[samples[k]];
+}
+
+int truth(Solver &S, const int64_t *samples, int64_t ns, double alpha, double *phi, double *g, cudaStream_t st) {
+    const int64_t n = S.n;
+    if (n <= 0 || ns <= 0) return TG_ERR_ARG;
+    if (alpha < 4.2) return TG_ERR_ARG;
+    for (int64_t k = 0; k < ns; k++)
+        if (samples[k] < 0 || samples[k] >= n) return TG_ERR_ARG;
+    /* reciprocal vectors, half space */
+    const double h2max = 38.0 * alpha * alpha / (M_PI * M_PI);
+    const int hmax = (int)std::sqrt(h2max) + 1;
+    std::vector<int4> hv;
+    for (int i = 0; i <= hmax; i++)
+        for (int j = -hmax; j <= hmax; j++)
+            for (int k = -hmax; k <= hmax; k++) {
+                if (i == 0 && (j < 0 || (j == 0 && k <= 0))) continue;
+                if ((double)(i * i + j * j + k * k) < h2max) hv.push_back(make_int4(i, j, k, 0));
+            }
+    const int nh = (int)hv.size();
+    DevBuf<int4> d_hv;
+    DevBuf<double> d_part, d_S, d_out;
+    DevBuf<int64_t> d_map, d_smp, d_sorted;
+    const int64_t chunk = 65536;
+    const int nchunks = (int)((n + chunk - 1) / chunk);
+    TG_TRY(ensure(d_hv, nh));
+    TG_TRY(ensure(d_part, 2 * (size_t)nh * nchunks));
+    TG_TRY(ensure(d_S, 2 * (size_t)nh));
+    TG_TRY(ensure(d_out, 4 * (size_t)ns));
+    TG_TRY(ensure(d_map, n));
+    TG_TRY(ensure(d_smp, ns));
+    TG_TRY(ensure(d_sorted, ns));
+    TG_CUDA(cudaMemcpyAsync(d_hv.p, hv.data(), sizeof(int4) * nh, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(d_smp.p, samples, sizeof(int64_t) * ns, cudaMemcpyHostToDevice, st));
+    k_find_sorted<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.pos.p, d_map.p);
+    k_pick<<<(int)((ns + 255) / 256), 256, 0, st>>>(d_map.p, d_smp.p, ns, d_sorted.p);
+    dim3 grid((nh + 255) / 256, nchunks);
+    k_sfac<<<grid, 256, 0, st>>>(n, S.pos.p, nh, d_hv.p, d_part.p, chunk);
+    k_sfac_reduce<<<(nh + 255) / 256, 256, 0, st>>>(nh, nchunks, d_part.p, d_S.p);
+    k_truth_real<<<(int)ns, 256, 0, st>>>(n, S.pos.p, d_sorted.p, ns, S.prm.m, S.prm.soft_len, alpha, d_out.p);
+    k_truth_four<<<(int)((ns + 127) / 128), 128, 0, st>>>(n, S.pos.p, d_sorted.p, ns, S.prm.m, alpha, nh, d_hv.p, d_S.p,
+                                                         d_out.p);
+    TG_CUDA(cudaGetLastError());
+    std::vector<double> h(4 * ns);
+    TG_CUDA(cudaMemcpyAsync(h.data(), d_out.p, sizeof(double) * 4 * ns, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    for (int64_t k = 0; k < ns; k++) {
+        if (phi) phi[k] = h[4 * k];
+        if (g)
+            for (int a = 0; a < 3; a++) g[3 * k + a] = h[4 * k + 1 + a];
+    }
+    release(d_hv);
+    release(d_part);
+    release(d_S);
+    release(d_out);
+    release(d_map);
+    release(d_smp);
+    release(d_sorted);
+    return TG_OK;
+}
+
+/* ---- FP32 FMA throughput: 8 independent FMA chains per thread ---- */
+__global__ void k_fma_peak(float *out, int iters, float a, float b) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = threadIdx.x * 1e-3f + k;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = fmaf(x[k], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 1.2345f) out[blockIdx.x] = s; /* keeps the chains live */
+}
+
+int fp32_peak(int device, double *tflops, cudaStream_t st) {
+    cudaDeviceProp prop;
+    TG_CUDA(cudaGetDeviceProperties(&prop, device));
+    const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 8192;
+    float *out = nullptr;
+    TG_CUDA(cudaMalloc(&out, sizeof(float) * blocks));
+    cudaEvent_t e0, e1;
+    TG_CUDA(cudaEventCreate(&e0));
+    TG_CUDA(cudaEventCreate(&e1));
+    k_fma_peak<<<blocks, threads, 0, st>>>(out, iters / 8, 0.999f, 1e-4f); /* warm-up */
+    TG_CUDA(cudaEventRecord(e0, st));
+    k_fma_peak<<<blocks, threads, 0, st>>>(out, iters, 0.999f, 1e-4f);
+    TG_CUDA(cudaEventRecord(e1, st));
+    TG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    TG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    return TG_OK;
+}
+
+} // namespace tg

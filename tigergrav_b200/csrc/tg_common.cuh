@@ -1,0 +1,508 @@
+/*
+ * tg_common.cuh -- shared device code: fixed-point positions, symmetric
+ * tensor storage, Green's-function derivatives, Ewald sums and the
+ * multipole/expansion contractions of the periodic gravity path.
+ *
+ * Storage layouts are the reference's (so node multipoles and expansions are
+ * interchangeable with it):
+ *   multipole (17): M, M_ab (6), M_abc (10)        tigergrav/multipole.hpp:24,58-82
+ *   expansion (35): L, L_a, L_ab, L_abc, L_abcd    tigergrav/expansion.hpp:28,77-137
+ * Within an order the slots enumerate sorted index tuples lexicographically.
+ */
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tg {
+
+constexpr int MP = 17;
+constexpr int LP = 35;
+constexpr double POS_MAX = 4294967296.0;
+constexpr double POS_INV = 1.0 / 4294967296.0;
+constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
+constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
+constexpr float EWALD_RCUT = 1.0e-6f;
+constexpr float EWALD_PHI0 = 2.8372975f; /* r -> 0 limit (tigergrav/green.hpp:272) */
+
+/* ---- symmetric index arithmetic (constant-folded after unrolling) ---- */
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a < b ? b : a; }
+/* index of sorted pair (p<=q) among sorted pairs of {0..n-1} */
+__host__ __device__ constexpr int idx2n(int p, int q, int n) { return p * n - p * (p - 1) / 2 + q - p; }
+/* number of sorted pairs of {k..n-1} summed over k < p */
+__host__ __device__ constexpr int off3n(int p, int n) {
+    return p == 0 ? 0 : (p == 1 ? n * (n + 1) / 2 : n * (n + 1) / 2 + (n - 1) * n / 2);
+}
+__host__ __device__ constexpr int idx3n(int p, int q, int r, int n) { return off3n(p, n) + idx2n(q - p, r - p, n - p); }
+/* number of sorted triples of {k..2} summed over k < p (n = 3) */
+__host__ __device__ constexpr int off4(int p) { return p == 0 ? 0 : (p == 1 ? 10 : 14); }
+
+__host__ __device__ constexpr int I2(int a, int b) { return idx2n(cmin(a, b), cmax(a, b), 3); }
+__host__ __device__ constexpr int I3(int a, int b, int c) {
+    return idx3n(cmin(a, cmin(b, c)), a + b + c - cmin(a, cmin(b, c)) - cmax(a, cmax(b, c)), cmax(a, cmax(b, c)), 3);
+}
+__host__ __device__ constexpr int sort4_0(int a, int b, int c, int d) { return cmin(cmin(a, b), cmin(c, d)); }
+__host__ __device__ constexpr int sort4_3(int a, int b, int c, int d) { return cmax(cmax(a, b), cmax(c, d)); }
+__host__ __device__ constexpr int sort4_1(int a, int b, int c, int d) {
+    /* second smallest */
+    return cmin(cmax(cmin(a, b), cmin(c, d)), cmin(cmax(a, b), cmax(c, d)));
+}
+__host__ __device__ constexpr int I4(int a, int b, int c, int d) {
+    return off4(sort4_0(a, b, c, d)) +
+           idx3n(sort4_1(a, b, c, d) - sort4_0(a, b, c, d),
+                 (a + b + c + d - sort4_0(a, b, c, d) - sort4_1(a, b, c, d) - sort4_3(a, b, c, d)) - sort4_0(a, b, c, d),
+                 sort4_3(a, b, c, d) - sort4_0(a, b, c, d), 3 - sort4_0(a, b, c, d));
+}
+__host__ __device__ constexpr int E0() { return 0; }
+__host__ __device__ constexpr int E1(int a) { return 1 + a; }
+__host__ __device__ constexpr int E2(int a, int b) { return 4 + I2(a, b); }
+__host__ __device__ constexpr int E3(int a, int b, int c) { return 10 + I3(a, b, c); }
+__host__ __device__ constexpr int E4(int a, int b, int c, int d) { return 20 + I4(a, b, c, d); }
+__host__ __device__ constexpr int M2(int a, int b) { return 1 + I2(a, b); }
+__host__ __device__ constexpr int M3(int a, int b, int c) { return 7 + I3(a, b, c); }
+
+/* expansion_factors (tigergrav/expansion.hpp:162-182): multiplicity / k!,
+ * accumulated in the working type exactly as the reference does; filled on
+ * the host by init_constants(); the library is one translation unit. */
+__constant__ float c_factor_f[LP];
+__constant__ double c_factor_d[LP];
+template <class T> __device__ __forceinline__ T factor(int i);
+template <> __device__ __forceinline__ float factor<float>(int i) { return c_factor_f[i]; }
+template <> __device__ __forceinline__ double factor<double>(int i) { return c_factor_d[i]; }
+
+/* ---- fixed point (tigergrav/position.hpp:18-37) ---- */
+__device__ __forceinline__ double pos2d(int32_t x) { return __dadd_rn(__dmul_rn((double)x, POS_INV), 0.5); }
+__device__ __forceinline__ int32_t d2pos(double x) {
+    const double y = __dadd_rn(x, -0.5);
+    long long z = llround(__dmul_rn(y, POS_MAX));
+    if ((double)z >= POS_MAX / 2.0) z -= (long long)POS_MAX;
+    return (int32_t)(uint32_t)(unsigned long long)z;
+}
+/* minimum-image separation of two fixed-point coordinates, in box units:
+ * (float)(int32)(X - Y) * 2^-32 (src/gravity.cpp:223) */
+__device__ __forceinline__ float wrap_sep_f(int32_t X, int32_t Y) {
+    return __int2float_rn((int32_t)((uint32_t)X - (uint32_t)Y)) * 2.3283064365386963e-10f;
+}
+__device__ __forceinline__ double wrap_sep_d(int32_t X, int32_t Y) {
+    return (double)(int32_t)((uint32_t)X - (uint32_t)Y) * POS_INV;
+}
+/* non-periodic separation (src/gravity.cpp:228) */
+__device__ __forceinline__ float free_sep_f(int32_t X, int32_t Y) {
+    return __ll2float_rn((long long)X - (long long)Y) * 2.3283064365386963e-10f;
+}
+__device__ __forceinline__ double free_sep_d(int32_t X, int32_t Y) {
+    return (double)((long long)X - (long long)Y) * POS_INV;
+}
+template <class T> __device__ __forceinline__ T sep(int32_t X, int32_t Y, bool periodic);
+template <> __device__ __forceinline__ float sep<float>(int32_t X, int32_t Y, bool periodic) {
+    return periodic ? wrap_sep_f(X, Y) : free_sep_f(X, Y);
+}
+template <> __device__ __forceinline__ double sep<double>(int32_t X, int32_t Y, bool periodic) {
+    return periodic ? wrap_sep_d(X, Y) : free_sep_d(X, Y);
+}
+
+template <class T> __device__ __forceinline__ T wrap_sep_t(int32_t X, int32_t Y);
+template <> __device__ __forceinline__ float wrap_sep_t<float>(int32_t X, int32_t Y) { return wrap_sep_f(X, Y); }
+template <> __device__ __forceinline__ double wrap_sep_t<double>(int32_t X, int32_t Y) { return wrap_sep_d(X, Y); }
+
+/* ---- per-type math ---- */
+__device__ __forceinline__ float t_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double t_rsqrt(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ float t_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double t_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float t_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double t_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ void t_sincospi(float x, float *s, float *c) { sincospif(x, s, c); }
+__device__ __forceinline__ void t_sincospi(double x, double *s, double *c) { sincospi(x, s, c); }
+
+/* erfc(x) and exp(-x^2).  FP32: the Abramowitz & Stegun 7.1.26 rational
+ * approximation that the reference uses (tigergrav/simd.hpp:676-692), with
+ * expf; FP64: the double-precision erfc and exp. */
+__device__ __forceinline__ float t_erfcexp(float x, float *e) {
+    const float t1 = __frcp_rn(1.0f + 0.3275911f * x);
+    *e = __expf(-x * x);
+    const float poly = t1 * (0.254829592f + t1 * (-0.284496736f + t1 * (1.421413741f + t1 * (-1.453152027f + t1 * 1.061405429f))));
+    return poly * *e;
+}
+__device__ __forceinline__ double t_erfcexp(double x, double *e) {
+    *e = exp(-x * x);
+    return erfc(x);
+}
+
+/* ---- Green's function derivatives ---- */
+
+/* green_deriv_direct (tigergrav/green.hpp:62-117): set D from radial factors */
+template <class T>
+__device__ __forceinline__ void green_deriv_set(T *D, T d0, T d1, T d2, T d3, T d4, const T *dx) {
+    D[E0()] = d0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E1(a)] = dx[a] * d1;
+#pragma unroll
+        for (int b = 0; b <= a; b++) {
+            const T dxadxb = dx[a] * dx[b];
+            D[E2(a, b)] = dxadxb * d2;
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                const T dxadxbdxc = dxadxb * dx[c];
+                D[E3(a, b, c)] = dxadxbdxc * d3;
+#pragma unroll
+                for (int d = 0; d <= c; d++) D[E4(a, b, c, d)] = dxadxbdxc * dx[d] * d4;
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E2(a, a)] += d1;
+        D[E3(a, a, a)] = fma(dx[a], d2, D[E3(a, a, a)]);
+        D[E4(a, a, a, a)] = fma(dx[a] * dx[a], d3, D[E4(a, a, a, a)]);
+        D[E4(a, a, a, a)] = fma(T(2), d2, D[E4(a, a, a, a)]);
+#pragma unroll
+        for (int b = 0; b <= a; b++) {
+            const T dxadxb = dx[a] * dx[b];
+            D[E3(a, a, b)] = fma(dx[b], d2, D[E3(a, a, b)]);
+            D[E3(a, b, b)] = fma(dx[a], d2, D[E3(a, b, b)]);
+            D[E4(a, a, a, b)] = fma(dxadxb, d3, D[E4(a, a, a, b)]);
+            D[E4(a, b, b, b)] = fma(dxadxb, d3, D[E4(a, b, b, b)]);
+            D[E4(a, a, b, b)] += d2;
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                D[E4(a, a, b, c)] = fma(dx[b], dx[c] * d3, D[E4(a, a, b, c)]);
+                D[E4(a, b, c, c)] = fma(dxadxb, d3, D[E4(a, b, c, c)]);
+                D[E4(a, b, b, c)] = fma(dx[a], dx[c] * d3, D[E4(a, b, b, c)]);
+            }
+        }
+    }
+}
+
+/* green_deriv_ewald (tigergrav/green.hpp:119-165): accumulate into D */
+template <class T, class A>
+__device__ __forceinline__ void green_deriv_add(A *D, T d0, T d1, T d2, T d3, T d4, const T *dx) {
+    D[E0()] += d0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E1(a)] += dx[a] * d1;
+        D[E2(a, a)] += d1;
+        D[E3(a, a, a)] += dx[a] * d2;
+        D[E4(a, a, a, a)] += dx[a] * dx[a] * d3;
+        D[E4(a, a, a, a)] += T(2) * d2;
+#pragma unroll
+        for (int b = 0; b <= a; b++) {
+            const T dxadxb = dx[a] * dx[b];
+            D[E2(a, b)] += dxadxb * d2;
+            D[E3(a, a, b)] += dx[b] * d2;
+            D[E3(a, b, b)] += dx[a] * d2;
+            D[E4(a, a, a, b)] += dxadxb * d3;
+            D[E4(a, b, b, b)] += dxadxb * d3;
+            D[E4(a, a, b, b)] += d2;
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                const T dxadxbdxc = dxadxb * dx[c];
+                D[E3(a, b, c)] += dxadxbdxc * d3;
+                D[E4(a, a, b, c)] += dx[b] * dx[c] * d3;
+                D[E4(a, b, c, c)] += dxadxb * d3;
+                D[E4(a, b, b, c)] += dx[a] * dx[c] * d3;
+#pragma unroll
+                for (int d = 0; d <= c; d++) D[E4(a, b, c, d)] += dxadxbdxc * dx[d] * d4;
+            }
+        }
+    }
+}
+
+/* green_direct (tigergrav/green.hpp:167-186) */
+template <class T>
+__device__ __forceinline__ void green_direct(const T *dX, T *D) {
+    const T r2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2];
+    const T rinv = (r2 > T(1.0e-18)) ? t_rsqrt(r2) : T(0);
+    const T r2inv = rinv * rinv;
+    const T d0 = -rinv;
+    const T d1 = -d0 * r2inv;
+    const T d2 = T(-3) * d1 * r2inv;
+    const T d3 = T(-5) * d2 * r2inv;
+    const T d4 = T(-7) * d3 * r2inv;
+    green_deriv_set(D, d0, d1, d2, d3, d4, dX);
+}
+
+/* Ewald tables (tigergrav/green.hpp:8-59), generated in FP64 on the device. */
+struct EwaldTables {
+    const float4 *real; /* NREAL lattice vectors n (w unused) */
+    const float4 *four; /* NFOUR reciprocal vectors h (w unused) */
+    const float *Hf;    /* NFOUR x 35 periodic_parts coefficients, float */
+    const double *Hd;   /* NFOUR x 35, double */
+};
+
+/* One real-space term of green_ewald (tigergrav/green.hpp:212-236), alpha = 2,
+ * masked at r >= 3.6.  Caller guarantees |X| > rcut (zmask = 1). */
+template <class T, class A>
+__device__ __forceinline__ void ewald_real_term(A *D, const T *X, float4 n) {
+    T dx[3] = {X[0] - T(n.x), X[1] - T(n.y), X[2] - T(n.z)};
+    const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+    if (!(r2 < T(12.96))) return;
+    const T rinv = t_rsqrt(r2);
+    const T r = r2 * rinv;
+    const T r2inv = rinv * rinv;
+    const T r3inv = r2inv * rinv;
+    const T r5inv = r2inv * r3inv;
+    const T r7inv = r2inv * r5inv;
+    const T r9inv = r2inv * r7inv;
+    const T r4 = r2 * r2;
+    T expfac;
+    const T erfc = t_erfcexp(T(2) * r, &expfac);
+    const T expfactor = T(2.2567583341910252) * r * expfac; /* 4/sqrt(pi) */
+    const T d0 = -erfc * rinv;
+    const T d1 = (expfactor + erfc) * r3inv;
+    const T d2 = -fma(expfactor, fma(T(8), r2, T(3)), T(3) * erfc) * r5inv;
+    const T d3 = fma(expfactor, (T(15) + fma(T(40), r2, T(64) * r4)), T(15) * erfc) * r7inv;
+    const T d4 = -fma(expfactor, fma(T(8) * r2, (T(35) + fma(T(56), r2, T(64) * r4)), T(105)), T(105) * erfc) * r9inv;
+    green_deriv_add<T, A>(D, d0, d1, d2, d3, d4, dx);
+}
+
+/* One reciprocal-space term of green_ewald (tigergrav/green.hpp:237-264). */
+template <class T, class A>
+__device__ __forceinline__ void ewald_four_term(A *D, const T *X, float4 h, const T *H) {
+    const T hdotdx = X[0] * T(h.x) + X[1] * T(h.y) + X[2] * T(h.z);
+    T si, co;
+    t_sincospi(T(2) * hdotdx, &si, &co);
+    D[E0()] += H[E0()] * co;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E1(a)] += H[E1(a)] * si;
+#pragma unroll
+        for (int b = 0; b <= a; b++) {
+            D[E2(a, b)] += H[E2(a, b)] * co;
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                D[E3(a, b, c)] += H[E3(a, b, c)] * si;
+#pragma unroll
+                for (int d = 0; d <= c; d++) D[E4(a, b, c, d)] += H[E4(a, b, c, d)] * co;
+            }
+        }
+    }
+}
+
+/* Final assembly of green_ewald (tigergrav/green.hpp:265-285) applied to a
+ * partial sum: adds pi/4 + 1/r and subtracts the direct derivatives.  Linear
+ * in D, so it may be applied to one lane's partial sum of a split evaluation. */
+template <class T, class A>
+__device__ __forceinline__ void ewald_finish(A *D, const T *X) {
+    T D1[LP];
+    green_direct<T>(X, D1);
+    D[E0()] += T(0.78539816339744831) - D1[E0()];
+#pragma unroll
+    for (int i = 1; i < LP; i++) D[i] -= D1[i];
+}
+
+/* ---- contractions (src/gravity.cpp:26-169) ---- */
+
+/* M2L: multipole M at dX -> expansion L (src/gravity.cpp:26-90) */
+template <class T, class A>
+__device__ __forceinline__ void contract_M2L(A *L, const T *M, const T *D) {
+    A L0 = M[0] * D[E0()];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = a; b < 3; b++) {
+            L0 += M[M2(a, b)] * D[E2(a, b)] * factor<T>(E2(a, b));
+#pragma unroll
+            for (int c = b; c < 3; c++) L0 -= M[M3(a, b, c)] * D[E3(a, b, c)] * factor<T>(E3(a, b, c));
+        }
+    L[E0()] += L0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        A La = M[0] * D[E1(a)];
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                La += M[M2(c, b)] * D[E3(a, b, c)] * factor<T>(E2(c, b));
+#pragma unroll
+                for (int d = c; d < 3; d++) La -= M[M3(b, c, d)] * D[E4(a, b, c, d)] * factor<T>(E3(b, c, d));
+            }
+        L[E1(a)] += La;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = a; b < 3; b++) {
+            A Lab = M[0] * D[E2(a, b)];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int d = c; d < 3; d++) Lab += M[M2(c, d)] * D[E4(a, b, c, d)] * factor<T>(E2(c, d));
+            L[E2(a, b)] += Lab;
+        }
+#pragma unroll
+    for (int i = 10; i < LP; i++) L[i] += M[0] * D[i];
+}
+
+/* P2L: point mass m at dX -> expansion L (src/gravity.cpp:92-121) */
+template <class T, class A>
+__device__ __forceinline__ void contract_P2L(A *L, T m, const T *D) {
+#pragma unroll
+    for (int i = 0; i < LP; i++) L[i] += m * D[i];
+}
+
+/* M2P: multipole M at dX -> potential and acceleration at a particle
+ * (src/gravity.cpp:123-169).  As in the reference, the potential's octupole
+ * sum runs a over all three axes (lines 141-147). */
+template <class T>
+__device__ __forceinline__ void contract_M2P(T &phi, T *g, const T *M, const T *D) {
+    T ffirst = M[0] * D[E0()];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = a; b < 3; b++) ffirst += M[M2(a, b)] * D[E2(a, b)] * factor<T>(E2(a, b));
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int c = b; c < 3; c++) ffirst -= M[M3(a, b, c)] * D[E3(a, b, c)] * factor<T>(E3(a, b, c));
+    phi = ffirst;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        T ga = -(M[0] * D[E1(a)]);
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                ga -= M[M2(c, b)] * D[E3(a, b, c)] * factor<T>(E2(c, b));
+#pragma unroll
+                for (int d = c; d < 3; d++) ga += M[M3(c, b, d)] * D[E4(a, b, c, d)] * factor<T>(E3(b, c, d));
+            }
+        g[a] = ga;
+    }
+}
+
+/* L2L: expansion<double>::operator<<= (tigergrav/expansion.hpp:184-233) */
+__device__ __forceinline__ void L2L(double *me, const double *dX) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        me[E0()] += me[E1(a)] * dX[a];
+#pragma unroll
+        for (int b = 0; b <= a; b++) {
+            me[E0()] += me[E2(a, b)] * dX[a] * dX[b] * c_factor_d[E2(a, b)];
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                me[E0()] += me[E3(a, b, c)] * dX[a] * dX[b] * dX[c] * c_factor_d[E3(a, b, c)];
+#pragma unroll
+                for (int d = 0; d <= c; d++)
+                    me[E0()] += me[E4(a, b, c, d)] * dX[a] * dX[b] * dX[c] * dX[d] * c_factor_d[E4(a, b, c, d)];
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            me[E1(a)] += me[E2(a, b)] * dX[b];
+#pragma unroll
+            for (int c = 0; c <= b; c++) {
+                me[E1(a)] += me[E3(a, b, c)] * dX[b] * dX[c] * c_factor_d[E2(b, c)];
+#pragma unroll
+                for (int d = 0; d <= c; d++) me[E1(a)] += me[E4(a, b, c, d)] * dX[b] * dX[c] * dX[d] * c_factor_d[E3(b, c, d)];
+            }
+        }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b <= a; b++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                me[E2(a, b)] += me[E3(a, b, c)] * dX[c];
+#pragma unroll
+                for (int d = 0; d <= c; d++) me[E2(a, b)] += me[E4(a, b, c, d)] * dX[c] * dX[d] * c_factor_d[E2(c, d)];
+            }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b <= a; b++)
+#pragma unroll
+            for (int c = 0; c <= b; c++)
+#pragma unroll
+                for (int d = 0; d < 3; d++) me[E3(a, b, c)] += me[E4(a, b, c, d)] * dX[d];
+}
+
+/* L2P: expansion<T>::translate_L2 (tigergrav/expansion.hpp:235-269) */
+template <class T>
+__device__ __forceinline__ void L2P(const T *me, const T *dX, T &phi, T *g) {
+    T p = me[E0()];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        p += me[E1(a)] * dX[a];
+#pragma unroll
+        for (int b = a; b < 3; b++) {
+            p += me[E2(a, b)] * dX[a] * dX[b] * factor<T>(E2(a, b));
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                p += me[E3(a, b, c)] * dX[a] * dX[b] * dX[c] * factor<T>(E3(a, b, c));
+#pragma unroll
+                for (int d = c; d < 3; d++) p += me[E4(a, b, c, d)] * dX[a] * dX[b] * dX[c] * dX[d] * factor<T>(E4(a, b, c, d));
+            }
+        }
+    }
+    phi = p;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        T ga = -me[E1(a)];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            ga -= me[E2(a, b)] * dX[b];
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                ga -= me[E3(a, b, c)] * dX[b] * dX[c] * factor<T>(E2(b, c));
+#pragma unroll
+                for (int d = c; d < 3; d++) ga -= me[E4(a, b, c, d)] * dX[b] * dX[c] * dX[d] * factor<T>(E3(b, c, d));
+            }
+        }
+        g[a] = ga;
+    }
+}
+
+/* M2M: multipole<float>::operator>>= (tigergrav/multipole.hpp:116-135) */
+__device__ __forceinline__ void M2M(float *me, const float *Y) {
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int q = p; q < 3; q++)
+#pragma unroll
+            for (int l = q; l < 3; l++) {
+                float m3 = me[M3(p, q, l)];
+                m3 = __fadd_rn(m3, __fmul_rn(__fmul_rn(__fmul_rn(me[0], Y[p]), Y[q]), Y[l]));
+                m3 = __fadd_rn(m3, __fmul_rn(me[M2(p, q)], Y[l]));
+                m3 = __fadd_rn(m3, __fmul_rn(me[M2(q, l)], Y[p]));
+                m3 = __fadd_rn(m3, __fmul_rn(me[M2(l, p)], Y[q]));
+                me[M3(p, q, l)] = m3;
+            }
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int q = p; q < 3; q++)
+            me[M2(p, q)] = __fadd_rn(me[M2(p, q)], __fmul_rn(__fmul_rn(me[0], Y[p]), Y[q]));
+}
+
+/* Kahan-compensated accumulator (FP32 path) */
+struct KahanF {
+    float s, c;
+    __device__ __forceinline__ void init() { s = 0.0f; c = 0.0f; }
+    __device__ __forceinline__ void add(float x) {
+        const float y = __fsub_rn(x, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ float value() const { return s - c; }
+};
+
+/* status flags written by kernels (never trap) */
+enum : uint32_t {
+    DEV_ERR_OVERFLOW_NEXT = 1u,
+    DEV_ERR_OVERFLOW_LIST = 2u,
+    DEV_ERR_OVERFLOW_SCRATCH = 4u,
+    DEV_ERR_DEPTH = 8u,
+    DEV_ERR_BADINDEX = 16u,
+    DEV_ERR_SPIN = 32u,
+};
+
+} // namespace tg

@@ -1,0 +1,7 @@
+/* Single translation unit of the library: the __constant__ tables of
+ * tg_aux.cu are visible to every kernel without relocatable device code. */
+#include "tg_aux.cu"
+#include "tg_tree.cu"
+#include "tg_walk.cu"
+#include "tg_gravity.cu"
+#include "tg_capi.cu"
