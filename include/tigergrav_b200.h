@@ -36,7 +36,8 @@ enum tg_status {
     TG_ERR_DEPTH = 4,    /* more than leaf_max particles share a 63-level box */
     TG_ERR_TIMEOUT = 5,  /* a bounded device wait ran out */
     TG_ERR_STATE = 6,    /* call out of order (e.g. forces before a build) */
-    TG_ERR_NOMEM = 7     /* device allocation failed */
+    TG_ERR_NOMEM = 7,    /* device allocation failed */
+    TG_ERR_SIZE = 8      /* n above what tg_energy_noalloc's fixed scratch holds */
 };
 
 enum tg_precision {
@@ -125,6 +126,19 @@ int tg_kick(tg_solver *s, double dt, void *stream);
 int tg_drift(tg_solver *s, double dt, void *stream);
 /* FP64 reductions: out[0] = E_kin, out[1] = E_pot (0.5 m phi G), out[2..4] = sum v / n. */
 int tg_energy(tg_solver *s, double out[5], void *stream);
+
+/* The same reductions over caller-owned device arrays, allocating nothing:
+ * for callers that cannot allocate device memory where they need the
+ * reduction (a fixed memory arena handed to the library up front, an
+ * allocation-free time loop).  No counterpart in the reference.
+ * v: n*3 floats, phi: n floats (NULL: E_pot = 0), out: 5 doubles, all device
+ * memory; n <= TG_NOALLOC_MAX_N, else TG_ERR_SIZE.  The partial sums live in a
+ * fixed 2.5 MiB array inside the library, shared by every call: calls that
+ * overlap on the GPU race.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+#define TG_NOALLOC_MAX_N (1ll << 26)
+int tg_energy_noalloc(const float *v, const float *phi, int64_t n, double m, double G, double *out,
+                      int device, void *stream);
 /* n_steps kick-drift-kick leapfrog steps of dt (first call computes forces if needed). */
 int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream);
 

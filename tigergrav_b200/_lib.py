@@ -12,7 +12,9 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtigergrav_b200.so")
 
-TG_OK, TG_ERR_ARG, TG_ERR_CUDA, TG_ERR_CAPACITY, TG_ERR_DEPTH, TG_ERR_TIMEOUT, TG_ERR_STATE, TG_ERR_NOMEM = range(8)
+TG_OK, TG_ERR_ARG, TG_ERR_CUDA, TG_ERR_CAPACITY, TG_ERR_DEPTH, TG_ERR_TIMEOUT, TG_ERR_STATE, TG_ERR_NOMEM, \
+    TG_ERR_SIZE = range(9)
+TG_NOALLOC_MAX_N = 1 << 26
 TG_PREC_F32, TG_PREC_F64 = 0, 1
 TG_HOST, TG_DEVICE = 0, 1
 LIST_KINDS = {"CC_D": 0, "CP_D": 1, "CC_E": 2, "CP_E": 3, "PC_D": 4, "PP_D": 5, "PC_E": 6, "PP_E": 7}
@@ -39,6 +41,7 @@ EXPORTS = [
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
+    "tg_energy_noalloc",
 ]
 
 
@@ -89,6 +92,7 @@ def _load():
     L.tg_gravity_CP_ewald.argtypes = [P(tg_params), i64, vp, vp, vp, vp, vp, vp]
     L.tg_truth.argtypes = [vp, vp, i64, d, vp, vp, vp]
     L.tg_device_fp32_peak.argtypes = [i32, P(d), vp]
+    L.tg_energy_noalloc.argtypes = [vp, vp, i64, d, d, vp, i32, vp]
     return L
 
 

@@ -231,6 +231,7 @@ const char *tg_error_string(int status) {
     case TG_ERR_TIMEOUT: return "bounded device wait timed out";
     case TG_ERR_STATE: return "call out of order";
     case TG_ERR_NOMEM: return "device allocation failed";
+    case TG_ERR_SIZE: return "n exceeds TG_NOALLOC_MAX_N (67108864), the capacity of tg_energy_noalloc's fixed scratch";
     default: return "unknown status";
     }
 }

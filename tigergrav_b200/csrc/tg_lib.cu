@@ -5,3 +5,4 @@
 #include "tg_walk.cu"
 #include "tg_gravity.cu"
 #include "tg_capi.cu"
+#include "tg_noalloc.cu"
