@@ -36,10 +36,14 @@ WORKLOADS = {
     "uniform32": dict(kind="uniform", n=32768, seed=1),
 }
 
-# FP32 operations executed per interaction by the leaf kernel (counted from
-# the source: separations 3, r^2 5, rsqrt 1, 1/r^3 2, sums 7 for PP; the
-# green_direct + M2P contraction for PC), used for the roofline numerator.
-EXEC_FLOPS = {"PP_D": 18, "PC_D": 330, "L2P": 0}
+# FP32 operations per PP pair in k_pp_f32's inner loop, counted from the
+# source with an FMA as 2: separation 9 (per axis two differences of split
+# coordinates and their sum), r^2 5 (1 mul + 2 fma), min 1, clamp 1,
+# rsqrt 1, 1/r^3 2, phi sum 1, three force FMAs 6 -> 26 (the Kahan fold,
+# ~1.3 per pair, is not counted).  Roofline numerator.
+EXEC_FLOPS = {"PP_D": 26}
+# DRAM bytes per PP pair of k_pp_f32 (ncu capture, filled in from profiles/)
+TRAFFIC_PP_BYTES_PER_PAIR = 0.0
 
 
 def make_particles(w):
@@ -199,7 +203,7 @@ def main():
         tdist.barrier()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    leaf_ms, launches0 = [], s.stats()["launches"]
+    pp_ms, launches0 = [], s.stats()["launches"]
     with ClockSampler(dev) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
@@ -208,7 +212,7 @@ def main():
             ev[k][1].record(stream)
             torch.cuda.synchronize()
             st = s.stats()
-            leaf_ms.append(st["ms"]["leaves"])
+            pp_ms.append(st["ms"]["pp"])
     torch.cuda.synchronize()
     launches = s.stats()["launches"] - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -223,10 +227,11 @@ def main():
     st = s.stats()
 
     # ---- end to end through the public API with host buffers ----
-    xh = np.ascontiguousarray(x)
-    vh = np.zeros((n, 3), np.float32)
-    phi_h = np.zeros(n, np.float32)
-    g_h = np.zeros((n, 3), np.float32)
+    # page-locked host buffers, as a production caller would hold them
+    xh = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+    vh = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
+    phi_h = torch.zeros(n, dtype=torch.float32).pin_memory()
+    g_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
     e2e_ms = []
     s2 = tg.GravitySolver(n, theta=args.theta, ewald=True, leaf_max=64, precision=args.precision, device=dev)
     for k in range(args.warmup + args.steps):
@@ -249,17 +254,20 @@ def main():
         tdist.all_reduce(t, op=tdist.ReduceOp.MIN)
         e2e_val = float(t.item())
 
-    # ---- roofline of the dominant kernel (the leaf kernel) ----
+    # ---- roofline of the dominant kernel (PP direct, k_pp_f32) ----
     peak = device_fp32_peak(dev)
     cnt = st["counts"]
-    exec_flops = cnt["PP_D"] * EXEC_FLOPS["PP_D"] + cnt["PC_D"] * EXEC_FLOPS["PC_D"]
-    leaf_s = float(np.mean(leaf_ms)) * 1e-3
-    achieved = exec_flops / leaf_s / 1e12
-    roof = {"kernel": "k_leaf<float,64> (L2P + PC + PP direct/Ewald)", "bound": "fp32", "achieved": achieved,
-            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-            "peak_source": "measured FMA kernel on this GPU (tg_device_fp32_peak)",
-            "flops_per_launch": exec_flops, "ms_per_launch": leaf_s * 1e3,
-            "phase_ms": st["ms"], "interactions": cnt,
+    pp_s = float(np.mean(pp_ms)) * 1e-3
+    exec_flops = cnt["PP_D"] * EXEC_FLOPS["PP_D"]
+    achieved = exec_flops / pp_s / 1e12 if pp_s > 0 else None
+    roof = {"kernel": "k_pp_f32 (PP direct, FP32)", "bound": "fp32", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if achieved else None,
+            "traffic": TRAFFIC_PP_BYTES_PER_PAIR * cnt["PP_D"],
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_pp_f32 on clustered64, "
+                              "scaled by PP pairs",
+            "peak_source": "measured FP32 FMA kernel on this GPU (tg_device_fp32_peak)",
+            "flops_per_launch": exec_flops, "flop_convention": "FP32 lane operations per PP pair (%d)" % EXEC_FLOPS["PP_D"],
+            "ms_per_launch": pp_s * 1e3, "phase_ms": st["ms"], "interactions": cnt,
             "ref_convention_gflop_per_eval": st["flops"] / 1e9}
 
     line = {"metric": "Mparticles/s per force eval (128^3 clustered, theta 0.7, Ewald)", "value": value,

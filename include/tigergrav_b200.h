@@ -84,6 +84,7 @@ typedef struct tg_stats {
     /* device time of the last solve, per phase, milliseconds */
     double ms_build, ms_multipoles, ms_walk, ms_nodes, ms_leaves, ms_kick_drift;
     int64_t launches;     /* kernels of this library launched on this handle so far */
+    double ms_pp;         /* part of ms_leaves spent in the FP32 PP-direct kernel (0 when it is not used) */
 } tg_stats;
 
 typedef struct tg_solver tg_solver;

@@ -30,7 +30,7 @@ class tg_stats(C.Structure):
                 ("walk_retries", C.c_int32), ("ref_stats", C.c_uint64 * 6), ("counts", C.c_uint64 * 8),
                 ("flops", C.c_double), ("ms_build", C.c_double), ("ms_multipoles", C.c_double),
                 ("ms_walk", C.c_double), ("ms_nodes", C.c_double), ("ms_leaves", C.c_double),
-                ("ms_kick_drift", C.c_double), ("launches", C.c_int64)]
+                ("ms_kick_drift", C.c_double), ("launches", C.c_int64), ("ms_pp", C.c_double)]
 
 
 # every symbol the header declares (checked by the CPU test suite)

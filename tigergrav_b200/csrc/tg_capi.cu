@@ -178,8 +178,24 @@ static int stage_host(Solver &S, size_t bytes) {
     return TG_OK;
 }
 
-/* copy a host buffer into a device buffer through pinned staging */
+/* true when the caller's host buffer is page-locked (cudaHostAlloc /
+ * cudaHostRegister): it is then copied directly, without staging */
+static bool is_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+/* copy a host buffer into a device buffer (pageable buffers through pinned staging) */
 static int h2d(Solver &S, void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    if (is_pinned(src)) {
+        TG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+        return TG_OK;
+    }
     TG_TRY(stage_host(S, bytes));
     std::memcpy(S.h_stage, src, bytes);
     TG_CUDA(cudaMemcpyAsync(dst, S.h_stage, bytes, cudaMemcpyHostToDevice, st));
@@ -187,6 +203,11 @@ static int h2d(Solver &S, void *dst, const void *src, size_t bytes, cudaStream_t
     return TG_OK;
 }
 static int d2h(Solver &S, void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    if (is_pinned(dst)) {
+        TG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+        return TG_OK;
+    }
     TG_TRY(stage_host(S, bytes));
     TG_CUDA(cudaMemcpyAsync(S.h_stage, src, bytes, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
@@ -516,6 +537,8 @@ int tg_get_stats(tg_solver *s, tg_stats *out) {
         phase_ms(S, 2, 3, &S.st.ms_walk);
         phase_ms(S, 3, 4, &S.st.ms_nodes);
         phase_ms(S, 4, 5, &S.st.ms_leaves);
+        S.st.ms_pp = 0.0;
+        if (S.pp_timed) phase_ms(S, 6, 5, &S.st.ms_pp);
     }
     S.st.launches = S.launches;
     *out = S.st;

@@ -232,13 +232,20 @@ struct EwaldTables {
     const double *Hd;   /* NFOUR x 35, double */
 };
 
-/* One real-space term of green_ewald (tigergrav/green.hpp:212-236), alpha = 2,
- * masked at r >= 3.6.  Caller guarantees |X| > rcut (zmask = 1). */
+/* Real-space cut of the Ewald sum.  The reference masks images at r >= 3.6
+ * (tigergrav/green.hpp:220); the FP64 path keeps that.  Images beyond
+ * r = 2.6 add at most 1.4e-7 (erfc(5.2) ~ 1e-12 times the derivative
+ * polynomials) to any r^k-scaled derivative -- below the FP32 rounding of the
+ * sums and below the 1.5e-7 error of the reference's own A&S erfc -- so the
+ * FP32 path stops there and evaluates ~80 images instead of ~200. */
+template <class T> __device__ __forceinline__ T ewald_rcut2();
+template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 6.76f; }
+template <> __device__ __forceinline__ double ewald_rcut2<double>() { return 12.96; }
+
+/* One real-space image of green_ewald (tigergrav/green.hpp:212-236), alpha = 2,
+ * at separation dx (|dx|^2 = r2 inside the cut). */
 template <class T, class A>
-__device__ __forceinline__ void ewald_real_term(A *D, const T *X, float4 n) {
-    T dx[3] = {X[0] - T(n.x), X[1] - T(n.y), X[2] - T(n.z)};
-    const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
-    if (!(r2 < T(12.96))) return;
+__device__ __forceinline__ void ewald_real_image(A *D, const T *dx, T r2) {
     const T rinv = t_rsqrt(r2);
     const T r = r2 * rinv;
     const T r2inv = rinv * rinv;
@@ -256,6 +263,39 @@ __device__ __forceinline__ void ewald_real_term(A *D, const T *X, float4 n) {
     const T d3 = fma(expfactor, (T(15) + fma(T(40), r2, T(64) * r4)), T(15) * erfc) * r7inv;
     const T d4 = -fma(expfactor, fma(T(8) * r2, (T(35) + fma(T(56), r2, T(64) * r4)), T(105)), T(105) * erfc) * r9inv;
     green_deriv_add<T, A>(D, d0, d1, d2, d3, d4, dx);
+}
+
+/* Visit the lattice images n of the reference's set (|n|^2 <= 17,
+ * tigergrav/green.hpp:3,8-28) with |X - n|^2 < ewald_rcut2, walking the
+ * integer ranges that the cut allows instead of testing all 305 vectors.
+ * fn(dx, r2, is_origin) is called once per image.  Caller guarantees
+ * |X| > 1e-6 (the reference's zmask = 1). */
+template <class T, class F>
+__device__ __forceinline__ void ewald_images(const T *X, F &&fn) {
+    const T R2 = ewald_rcut2<T>();
+    const T R = t_sqrt(R2);
+    const int nx0 = (int)ceil(X[0] - R), nx1 = (int)floor(X[0] + R);
+    for (int nx = nx0; nx <= nx1; nx++) {
+        const T dx = X[0] - T(nx);
+        const T rx = R2 - dx * dx;
+        if (!(rx > T(0))) continue;
+        const T ry = t_sqrt(rx);
+        const int ny0 = (int)ceil(X[1] - ry), ny1 = (int)floor(X[1] + ry);
+        for (int ny = ny0; ny <= ny1; ny++) {
+            const T dy = X[1] - T(ny);
+            const T rxy = rx - dy * dy;
+            if (!(rxy > T(0))) continue;
+            const T rz = t_sqrt(rxy);
+            const int nz0 = (int)ceil(X[2] - rz), nz1 = (int)floor(X[2] + rz);
+            for (int nz = nz0; nz <= nz1; nz++) {
+                if (nx * nx + ny * ny + nz * nz > 17) continue;
+                const T d[3] = {dx, dy, X[2] - T(nz)};
+                const T r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                if (!(r2 < R2)) continue;
+                fn(d, r2, nx == 0 && ny == 0 && nz == 0);
+            }
+        }
+    }
 }
 
 /* One reciprocal-space term of green_ewald (tigergrav/green.hpp:237-264). */

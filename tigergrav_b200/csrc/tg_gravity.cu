@@ -2,15 +2,18 @@
  * tg_gravity.cu -- the interaction kernels of kick_fmm (src/tree.cpp:400-631)
  * and the eight kernel-level seams of tigergrav/gravity.hpp:39-46.
  *
- *   k_node   one warp per node: CC/CP direct (lanes over sources) and
- *            CC/CP Ewald (lanes split the 305 real + 123 reciprocal terms of
- *            each source's green_ewald; the contraction is linear, so each
- *            lane contracts its partial derivative sum) -> Lloc (35 doubles)
+ *   k_node   one warp per node, lanes over sources: CC/CP direct and
+ *            CC/CP Ewald (one thread evaluates a source's whole green_ewald,
+ *            walking only the lattice images inside the real-space cut, then
+ *            contracts it); lane sums are reduced in FP64 -> Lloc (35 doubles)
  *   k_l2l    one thread per node of a level, top-down:
  *            L = (L_parent << (x - x_parent)) + Lloc          (FP64)
  *   k_leaf   one block per leaf, one thread per sink particle: L2P, then
  *            PC_direct, PP_direct (source leaves staged in shared memory),
  *            PC_ewald, PP_ewald; -phi_self once (src/gravity.cpp:295).
+ *            The FP32 path with leaf_max <= 64 runs it without PP_direct
+ *            (into an FP64 buffer) and then k_pp_f32 (tg_pp.cuh), which adds
+ *            PP_direct and phi_self and writes the float4 result.
  *
  * Precision: T = float (FP32 path: FP32 arithmetic, per-tile FP32 partial
  * sums folded into Kahan-compensated accumulators) or T = double (the plain
@@ -137,7 +140,7 @@ __device__ __forceinline__ void ewald_nearest(T r, T rinv, T &p0, T &f0) {
 }
 
 /* ---- PP Ewald pair (src/gravity.cpp:533-603): phi and g of the periodic
- * correction per unit mass.  The lattice table's last entry is n = 0. */
+ * correction per unit mass.  The n = 0 image is taken by ewald_nearest. */
 template <class T>
 __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0, T &phi, T *g) {
     const T r2 = dX0[0] * dX0[0] + dX0[1] * dX0[1] + dX0[2] * dX0[2];
@@ -147,11 +150,9 @@ __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0
         return;
     }
     T ph = T(0), gx = T(0), gy = T(0), gz = T(0);
-    for (int t = 0; t < NREAL - 1; t++) {
-        const float4 n = __ldg(&E.real[t]);
-        const T dx = dX0[0] - T(n.x), dy = dX0[1] - T(n.y), dz = dX0[2] - T(n.z);
-        const T rr2 = dx * dx + dy * dy + dz * dz;
-        if (!(rr2 < T(12.96))) continue;
+    ewald_images<T>(dX0, [&](const T *d, T rr2, bool origin) {
+        if (origin) return;
+        const T dx = d[0], dy = d[1], dz = d[2];
         const T rinv = t_rsqrt(rr2);
         const T r = rr2 * rinv;
         T expfac;
@@ -163,7 +164,7 @@ __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0
         gx -= dx * d1;
         gy -= dy * d1;
         gz -= dz * d1;
-    }
+    });
     for (int t = 0; t < NFOUR; t++) {
         const float4 h = __ldg(&E.four[t]);
         const T hdotdx = dX0[0] * T(h.x) + dX0[1] * T(h.y) + dX0[2] * T(h.z);
@@ -194,30 +195,12 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
         D[0] = T(EWALD_PHI0);
         return;
     }
-    for (int t = 0; t < NREAL; t++) ewald_real_term<T, T>(D, X, __ldg(&E.real[t]));
+    ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T, T>(D, d, rr2); });
     for (int t = 0; t < NFOUR; t++) {
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
         ewald_four_term<T, T>(D, X, __ldg(&E.four[t]), H);
     }
     ewald_finish<T, T>(D, X);
-}
-
-/* partial green_ewald for a warp: this lane's share of the terms */
-template <class T>
-__device__ __forceinline__ void green_ewald_lane(const EwaldTables &E, const T *X, T *D, int lane) {
-#pragma unroll
-    for (int k = 0; k < LP; k++) D[k] = T(0);
-    const T r2 = X[0] * X[0] + X[1] * X[1] + X[2] * X[2];
-    if (!(r2 > T(1.0e-12))) {
-        if (lane == 0) D[0] = T(EWALD_PHI0);
-        return;
-    }
-    for (int t = lane; t < NREAL; t += 32) ewald_real_term<T, T>(D, X, __ldg(&E.real[t]));
-    for (int t = lane; t < NFOUR; t += 32) {
-        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
-        ewald_four_term<T, T>(D, X, __ldg(&E.four[t]), H);
-    }
-    if (lane == 0) ewald_finish<T, T>(D, X);
 }
 
 struct ListView {
@@ -284,14 +267,14 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
             /* CC Ewald (src/gravity.cpp:680-731) */
             const int32_t *lst = LV.pool[TG_CC_E] + LV.off[TG_CC_E][i];
             const int32_t len = LV.len[TG_CC_E][i];
-            for (int32_t j = 0; j < len; j++) {
+            for (int32_t j = lane; j < len; j += 32) {
                 const MSrc &s = ms[lst[j]];
                 T dX[3], D[LP], M[MP];
 #pragma unroll
                 for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
 #pragma unroll
                 for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-                green_ewald_lane<T>(E, dX, D, lane);
+                green_ewald_full<T>(E, dX, D);
                 contract_M2L<T, T>(L, M, D);
             }
             /* CP Ewald (src/gravity.cpp:733-785) */
@@ -300,13 +283,13 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
             const T m = T(P.m_d);
             for (int32_t c = 0; c < ncp; c++) {
                 const int32_t src = lcp[c];
-                for (int32_t q = pb[src]; q < pe[src]; q++) {
+                for (int32_t q = pb[src] + lane; q < pe[src]; q += 32) {
                     const int4 y = pos[q];
                     const int32_t yy[3] = {y.x, y.y, y.z};
                     T dX[3], D[LP];
 #pragma unroll
                     for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], yy[d], true);
-                    green_ewald_lane<T>(E, dX, D, lane);
+                    green_ewald_full<T>(E, dX, D);
                     contract_P2L<T, T>(L, m, D);
                 }
             }
@@ -346,7 +329,7 @@ __global__ void k_l2l(int64_t first, int64_t count, const int32_t *__restrict__ 
 }
 
 /* ---- leaf kernel ---- */
-template <class T, int BLOCK>
+template <class T, int BLOCK, bool PP = true>
 __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
                                                 const int32_t *__restrict__ pb, const int32_t *__restrict__ pe,
                                                 const MSrc *__restrict__ ms, const int4 *__restrict__ pos, ListView LV,
@@ -394,7 +377,7 @@ __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__rest
             }
         }
         /* PP direct (src/gravity.cpp:171-300) */
-        {
+        if (PP) {
             const int32_t *lst = LV.pool[TG_PP_D] + LV.off[TG_PP_D][leaf];
             const int32_t len = LV.len[TG_PP_D][leaf];
             const T m = T(P.m_d);
@@ -469,7 +452,7 @@ __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__rest
             }
         }
         if (active) {
-            const double phi = aphi.get() - P.phi_self;
+            const double phi = aphi.get() - (PP ? P.phi_self : 0.0);
             if (acc_f) acc_f[b + tid] = make_float4((float)phi, (float)ag[0].get(), (float)ag[1].get(), (float)ag[2].get());
             if (acc_d) {
                 acc_d[4 * (int64_t)(b + tid) + 0] = phi;
@@ -478,6 +461,47 @@ __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__rest
         }
     }
 }
+
+/* ---- PP direct for the FP32 path (leaf_max <= 64) ----
+ * Source positions are staged in split fixed point relative to the sink
+ * leaf's centre Xr: for a = wrap(Y - Xr),
+ *     hi = (a >> 16) 2^-16,   lo = (a & 0xffff) 2^-32
+ * are exact in FP32, and dX = (hi_i - hi_j) + (lo_i - lo_j) is the correctly
+ * rounded FP32 value of (X_i - Y_j) 2^-32 -- exactly the reference's dX
+ * (src/gravity.cpp:223) -- from three FP32 additions and no integer-to-float
+ * conversion per pair.  The identity needs |a_i - a_j| < 2^31, checked per
+ * staged batch; otherwise that batch's pairs take the per-pair wrap. */
+struct __align__(16) SrcHL {
+    float hx, hy, hz, hpad;
+    float lx, ly, lz, lpad;
+};
+
+__device__ __forceinline__ void split_hl(int32_t a, float &h, float &l) {
+    h = __int2float_rn(a >> 16) * 1.52587890625e-05f;
+    l = __int2float_rn(a & 0xffff) * 2.3283064365386963e-10f;
+}
+
+__device__ __forceinline__ uint32_t warp_max_u(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+/* offset of Y from Xr: int32 wrap (periodic) or plain difference (free space);
+ * mag accumulates the largest magnitude, saturated at 2^30 */
+__device__ __forceinline__ int32_t rel_off(int32_t Y, int32_t Xr, bool per, uint32_t &mag) {
+    if (per) {
+        const int32_t a = (int32_t)((uint32_t)Y - (uint32_t)Xr);
+        mag = max(mag, (uint32_t)abs(a));
+        return a;
+    }
+    const long long a = (long long)Y - (long long)Xr;
+    const unsigned long long aa = (unsigned long long)(a < 0 ? -a : a);
+    mag = max(mag, aa >= (1ull << 30) ? (1u << 30) : (uint32_t)aa);
+    return (int32_t)a;
+}
+
+#include "tg_pp.cuh"
 
 /* ---------------- kernel-level seams ---------------- */
 
@@ -540,7 +564,7 @@ __global__ void k_seam_pc(GParams P, int kind_ewald, int64_t ngroups, const int6
     }
 }
 
-/* CC/CP seams: one warp per group (lanes split sources, or Ewald terms) */
+/* CC/CP seams: one warp per group, lanes over sources */
 template <class T>
 __global__ void k_seam_node(GParams P, int kind_ewald, int is_cc, int64_t ngroups, const int32_t *__restrict__ sink_x,
                             const int64_t *__restrict__ src_off, const float *__restrict__ src_m,
@@ -553,31 +577,17 @@ __global__ void k_seam_node(GParams P, int kind_ewald, int is_cc, int64_t ngroup
         T L[LP];
         for (int k = 0; k < LP; k++) L[k] = T(0);
         const int64_t b = src_off[g], e = src_off[g + 1];
-        if (!kind_ewald) {
-            for (int64_t j = b + lane; j < e; j += 32) {
-                T dX[3], D[LP];
-                for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], src_x[3 * j + d], per);
-                green_direct<T>(dX, D);
-                if (is_cc) {
-                    T M[MP];
-                    for (int q = 0; q < MP; q++) M[q] = T(src_m[MP * j + q]);
-                    contract_M2L<T, T>(L, M, D);
-                } else {
-                    contract_P2L<T, T>(L, T(P.m_d), D);
-                }
-            }
-        } else {
-            for (int64_t j = b; j < e; j++) {
-                T dX[3], D[LP];
-                for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], src_x[3 * j + d], true);
-                green_ewald_lane<T>(E, dX, D, lane);
-                if (is_cc) {
-                    T M[MP];
-                    for (int q = 0; q < MP; q++) M[q] = T(src_m[MP * j + q]);
-                    contract_M2L<T, T>(L, M, D);
-                } else {
-                    contract_P2L<T, T>(L, T(P.m_d), D);
-                }
+        for (int64_t j = b + lane; j < e; j += 32) {
+            T dX[3], D[LP];
+            for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], src_x[3 * j + d], per);
+            if (kind_ewald) green_ewald_full<T>(E, dX, D);
+            else green_direct<T>(dX, D);
+            if (is_cc) {
+                T M[MP];
+                for (int q = 0; q < MP; q++) M[q] = T(src_m[MP * j + q]);
+                contract_M2L<T, T>(L, M, D);
+            } else {
+                contract_P2L<T, T>(L, T(P.m_d), D);
             }
         }
         for (int k = 0; k < LP; k++) {
@@ -611,8 +621,10 @@ int gravity_forces(Solver &S, cudaStream_t st) {
     const bool f64 = S.prm.precision == TG_PREC_F64;
     TG_TRY(ensure(S.nd_Lloc, 35 * nn));
     TG_TRY(ensure(S.nd_L, 35 * nn));
-    if (f64) TG_TRY(ensure(S.accd, 4 * n));
-    else TG_TRY(ensure(S.acc, n));
+    const bool split_pp = !f64 && S.prm.leaf_max <= 64;
+    if (f64 || split_pp) TG_TRY(ensure(S.accd, 4 * n));
+    if (!f64) TG_TRY(ensure(S.acc, n));
+    S.pp_timed = false;
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[3], st));
     {
         const int TPB = 128;
@@ -639,9 +651,18 @@ int gravity_forces(Solver &S, cudaStream_t st) {
             if (f64)
                 k_leaf<double, 64><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV, E,
                                                      S.nd_L.p, nullptr, S.accd.p);
-            else
-                k_leaf<float, 64><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV, E,
-                                                    S.nd_L.p, S.acc.p, nullptr);
+            else {
+                /* far part in FP64, then PP direct over the same leaves */
+                k_leaf<float, 64, false><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
+                                                           S.pos.p, LV, E, S.nd_L.p, nullptr, S.accd.p);
+                TG_TRY(launched(S));
+                if (S.have_events) {
+                    TG_CUDA(cudaEventRecord(S.ev[6], st));
+                    S.pp_timed = true;
+                }
+                k_pp_f32<2><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                              S.accd.p, S.acc.p);
+            }
         } else {
             if (f64)
                 k_leaf<double, 128><<<g, 128, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,

@@ -118,6 +118,7 @@ struct Solver {
     /* events for phase timing */
     cudaEvent_t ev[8];
     bool have_events = false;
+    bool pp_timed = false; /* ev[6] marks the start of the FP32 PP kernel in the last solve */
     tg_stats st{};
     int num_sms = 148;
     int64_t launches = 0; /* kernels of this library launched on this handle */

@@ -40,6 +40,9 @@ def _ptr(a):
     if _is_torch_cuda(a):
         assert a.is_contiguous()
         return C.c_void_p(a.data_ptr()), TG_DEVICE
+    if hasattr(a, "data_ptr"):  # torch CPU tensor (pinned ones are copied without staging)
+        assert a.is_contiguous()
+        return C.c_void_p(a.data_ptr()), TG_HOST
     assert isinstance(a, np.ndarray) and a.flags.c_contiguous
     return C.c_void_p(a.ctypes.data), TG_HOST
 
@@ -168,7 +171,7 @@ class GravitySolver:
         return dict(n=s.n, nodes=s.nodes, leaves=s.leaves, depth=s.depth, walk_retries=s.walk_retries,
                     ref_stats=dict(zip(refk, map(int, s.ref_stats))), counts=dict(zip(kinds, map(int, s.counts))),
                     flops=s.flops, launches=s.launches, ms=dict(build=s.ms_build, multipoles=s.ms_multipoles, walk=s.ms_walk,
-                                           nodes=s.ms_nodes, leaves=s.ms_leaves))
+                                           nodes=s.ms_nodes, leaves=s.ms_leaves, pp=s.ms_pp))
 
     # ---- introspection ----
     @property
