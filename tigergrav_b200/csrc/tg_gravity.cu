@@ -471,11 +471,6 @@ __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__rest
  * (src/gravity.cpp:223) -- from three FP32 additions and no integer-to-float
  * conversion per pair.  The identity needs |a_i - a_j| < 2^31, checked per
  * staged batch; otherwise that batch's pairs take the per-pair wrap. */
-struct __align__(16) SrcHL {
-    float hx, hy, hz, hpad;
-    float lx, ly, lz, lpad;
-};
-
 __device__ __forceinline__ void split_hl(int32_t a, float &h, float &l) {
     h = __int2float_rn(a >> 16) * 1.52587890625e-05f;
     l = __int2float_rn(a & 0xffff) * 2.3283064365386963e-10f;
@@ -660,8 +655,8 @@ int gravity_forces(Solver &S, cudaStream_t st) {
                     TG_CUDA(cudaEventRecord(S.ev[6], st));
                     S.pp_timed = true;
                 }
-                k_pp_f32<2><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
-                                              S.accd.p, S.acc.p);
+                k_pp_f32<<<2 * g, 32, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                               S.accd.p, S.acc.p);
             }
         } else {
             if (f64)
