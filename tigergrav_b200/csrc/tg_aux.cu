@@ -102,7 +102,11 @@ int ewald_tables(Solver &S, cudaStream_t st) {
     const auto real = lattice(17), four = lattice(9);
     if ((int)real.size() != NREAL || (int)four.size() != NFOUR) return TG_ERR_STATE;
     std::vector<float4> r4(NREAL), f4(NFOUR);
-    for (int i = 0; i < NREAL; i++) r4[i] = make_float4((float)real[i][0], (float)real[i][1], (float)real[i][2], 0.0f);
+    /* device order: increasing |n|^2, so the first NREAL_F32 are the candidates of the FP32 cut */
+    for (int i = 0; i < NREAL; i++) {
+        const auto &v = real[NREAL - 1 - i];
+        r4[i] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    }
     for (int i = 0; i < NFOUR; i++) f4[i] = make_float4((float)four[i][0], (float)four[i][1], (float)four[i][2], 0.0f);
     TG_TRY(ensure(S.ew_real, NREAL));
     TG_TRY(ensure(S.ew_four, NFOUR));

@@ -21,6 +21,7 @@ constexpr int LP = 35;
 constexpr double POS_MAX = 4294967296.0;
 constexpr double POS_INV = 1.0 / 4294967296.0;
 constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
+constexpr int NREAL_F32 = 179; /* |n|^2 <= 12: every n that can lie within the FP32 cut 2.6 of |X| <= sqrt(3)/2 */
 constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
 constexpr float EWALD_RCUT = 1.0e-6f;
 constexpr float EWALD_PHI0 = 2.8372975f; /* r -> 0 limit (tigergrav/green.hpp:272) */
@@ -226,7 +227,7 @@ __device__ __forceinline__ void green_direct(const T *dX, T *D) {
 
 /* Ewald tables (tigergrav/green.hpp:8-59), generated in FP64 on the device. */
 struct EwaldTables {
-    const float4 *real; /* NREAL lattice vectors n (w unused) */
+    const float4 *real; /* NREAL lattice vectors n by increasing |n|^2 (w = |n|^2) */
     const float4 *four; /* NFOUR reciprocal vectors h (w unused) */
     const float *Hf;    /* NFOUR x 35 periodic_parts coefficients, float */
     const double *Hd;   /* NFOUR x 35, double */

@@ -203,6 +203,33 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
     ewald_finish<T, T>(D, X);
 }
 
+/* green_ewald(dX) split over a warp: this lane's share of the real-space
+ * candidates (every n that can fall inside the cut) and of the reciprocal
+ * terms, plus, on lane 0, the final assembly.  The sum of the 32 partial
+ * results is green_ewald; the M2L / P2L contractions are linear, so each lane
+ * contracts its own part.  X must not be 0 (the caller handles r <= 1e-6). */
+template <class T>
+__device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *X, T *D, int lane) {
+#pragma unroll
+    for (int k = 0; k < LP; k++) D[k] = T(0);
+    const int ncand = sizeof(T) == 4 ? NREAL_F32 : NREAL;
+    for (int t = lane; t < ncand; t += 32) {
+        const float4 n = __ldg(&E.real[t]);
+        const T dx[3] = {X[0] - T(n.x), X[1] - T(n.y), X[2] - T(n.z)};
+        const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+        if (r2 < ewald_rcut2<T>()) ewald_real_image<T, T>(D, dx, r2);
+    }
+    for (int t = lane; t < NFOUR; t += 32) {
+        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
+        ewald_four_term<T, T>(D, X, __ldg(&E.four[t]), H);
+    }
+    if (lane == 0) ewald_finish<T, T>(D, X);
+}
+
+/* CC/CP Ewald lists shorter than this are evaluated one source at a time by
+ * the whole warp (green_ewald_warp); longer ones one source per lane */
+constexpr int EWALD_WARP_LIST = 12;
+
 struct ListView {
     int32_t *pool[NLIST];
     int64_t *off[NLIST];
@@ -267,15 +294,33 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
             /* CC Ewald (src/gravity.cpp:680-731) */
             const int32_t *lst = LV.pool[TG_CC_E] + LV.off[TG_CC_E][i];
             const int32_t len = LV.len[TG_CC_E][i];
-            for (int32_t j = lane; j < len; j += 32) {
-                const MSrc &s = ms[lst[j]];
-                T dX[3], D[LP], M[MP];
+            if (len >= EWALD_WARP_LIST) {
+                for (int32_t j = lane; j < len; j += 32) {
+                    const MSrc &s = ms[lst[j]];
+                    T dX[3], D[LP], M[MP];
 #pragma unroll
-                for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
+                    for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
 #pragma unroll
-                for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-                green_ewald_full<T>(E, dX, D);
-                contract_M2L<T, T>(L, M, D);
+                    for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
+                    green_ewald_full<T>(E, dX, D);
+                    contract_M2L<T, T>(L, M, D);
+                }
+            } else {
+                for (int32_t j = 0; j < len; j++) {
+                    const MSrc &s = ms[lst[j]];
+                    T dX[3], D[LP], M[MP];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
+                    if (!(dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2] > T(1.0e-12))) {
+                        /* the node itself: green_ewald(0) = phi0 only (tigergrav/green.hpp:279) */
+                        if (lane == 0) L[E0()] += T(s.m[0]) * T(EWALD_PHI0);
+                        continue;
+                    }
+#pragma unroll
+                    for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
+                    green_ewald_warp<T>(E, dX, D, lane);
+                    contract_M2L<T, T>(L, M, D);
+                }
             }
             /* CP Ewald (src/gravity.cpp:733-785) */
             const int32_t *lcp = LV.pool[TG_CP_E] + LV.off[TG_CP_E][i];
