@@ -66,6 +66,7 @@ def lib():
         L.tgo_get_forces.argtypes = [vp, vp, vp]
         L.tgo_get_expansions.argtypes = [vp, vp]
         L.tgo_get_stats.argtypes = [vp, vp, vp, vp]
+        L.tgo_kind_costs.argtypes = [vp, i32, i32, C.c_double, C.c_uint64, vp, vp]
         L.tgo_kick.argtypes = [vp, C.c_double]
         L.tgo_drift.argtypes = [vp, C.c_double, vp]
         L.tgo_get_particles.argtypes = [vp, vp, vp]
@@ -339,6 +340,23 @@ class Oracle:
         ref = dict(zip(("PP_direct", "PP_ewald", "CC_direct", "CC_ewald", "CP_direct", "CP_ewald"), map(int, rs)))
         clean = dict(zip(("PP_D", "PP_E", "PC_D", "PC_E", "CC_D", "CC_E", "CP_D", "CP_E"), map(int, cnt)))
         return ref, clean, int(fl[0])
+
+    def kind_costs(self, use_ref=True, nthreads=0, budget_s=1.0, seed=1):
+        """Host throughput per interaction kind: {kind: (ns per interaction, interactions sampled)}
+        (each kind's kernel alone over random sinks for at most budget_s seconds; after walk())."""
+        if use_ref:
+            if ref_lib() is None:
+                raise RuntimeError("reference kernels not built (oracle/_ref)")
+            rc = lib().tgo_load_reference(self.h, REF_PATH.encode())
+            if rc != 0:
+                raise RuntimeError("tgo_load_reference: %d" % rc)
+        ns = np.zeros(8)
+        done = np.zeros(8, np.uint64)
+        nt = nthreads or os.cpu_count() or 1
+        rc = lib().tgo_kind_costs(self.h, 1 if use_ref else 0, nt, float(budget_s), int(seed), _p(ns), _p(done))
+        if rc != 0:
+            raise RuntimeError("tgo_kind_costs: %d" % rc)
+        return {k: (float(ns[v]), int(done[v])) for k, v in KINDS.items()}
 
     def kick(self, dt):
         assert lib().tgo_kick(self.h, dt) == 0

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <dlfcn.h>
 #include <thread>
+#include <chrono>
 #include <vector>
 
 namespace {
@@ -1055,6 +1056,99 @@ int tgo_evaluate(void *h, int use_ref, int nthreads, const int32_t *leaf_subset,
         }
         S.flops += fl;
     });
+    return 0;
+}
+
+/* Throughput of each interaction kind on the host, for the CPU baseline of a
+ * workload too large to evaluate in full: for kind k (TGO_CC_D ... TGO_PP_E)
+ * the kernel of that kind alone runs over randomly chosen sinks with a
+ * non-empty list of that kind, on nthreads threads, until budget_s seconds or
+ * all such sinks are done.  ns_per[k] = wall ns / interactions evaluated
+ * (interactions counted as in tgo_get_stats), done[k] = interactions
+ * evaluated.  A whole evaluation then costs about sum_k count_k * ns_per[k]. */
+int tgo_kind_costs(void *h, int use_ref, int nthreads, double budget_s, uint64_t seed, double *ns_per, uint64_t *done) {
+    Solver &S = *(Solver *)h;
+    if (use_ref == 1 && !S.dl) return -1;
+    const size_t nn = S.nodes.size();
+    if (S.lists[0].size() != nn) return -2; /* no walk yet */
+    const int nt = nthreads > 0 ? nthreads : 1;
+    for (int kind = 0; kind < TGO_NLIST; kind++) {
+        ns_per[kind] = 0.0;
+        done[kind] = 0;
+        std::vector<int32_t> sinks;
+        for (size_t i = 0; i < nn; i++)
+            if (!S.lists[kind][i].empty() && S.nodes[i].pe > S.nodes[i].pb) sinks.push_back((int32_t)i);
+        if (sinks.empty()) continue;
+        uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull + (uint64_t)kind;
+        for (size_t a = sinks.size() - 1; a > 0; a--) { /* Fisher-Yates */
+            st = st * 6364136223846793005ull + 1442695040888963407ull;
+            std::swap(sinks[a], sinks[(size_t)((st >> 33) % (a + 1))]);
+        }
+        const bool node_kind = kind == TGO_CC_D || kind == TGO_CP_D || kind == TGO_CC_E || kind == TGO_CP_E;
+        std::atomic<int64_t> next{0};
+        std::atomic<uint64_t> work{0};
+        std::atomic<bool> stop{false};
+        const auto t0 = std::chrono::steady_clock::now();
+        auto body = [&]() {
+            std::vector<float> ym;
+            std::vector<int32_t> yx, y;
+            std::vector<double> f, L(LP);
+            for (;;) {
+                if (stop.load(std::memory_order_relaxed)) break;
+                const int64_t k = next.fetch_add(1);
+                if (k >= (int64_t)sinks.size()) break;
+                const Node &nd = S.nodes[sinks[k]];
+                const auto &lst = S.lists[kind][sinks[k]];
+                const int nx = (int)(nd.pe - nd.pb);
+                const int32_t *xs = &S.x[3 * nd.pb];
+                uint64_t w = 0;
+                if (node_kind) {
+                    std::fill(L.begin(), L.end(), 0.0);
+                    if (kind == TGO_CC_D || kind == TGO_CC_E) {
+                        gather_multi(S, lst, ym, yx);
+                        if (use_ref == 1)
+                            (kind == TGO_CC_D ? S.ref_cc_d : S.ref_cc_e)(&S.p, L.data(), nd.x, ym.data(), yx.data(), (int)lst.size());
+                        else
+                            (kind == TGO_CC_D ? tgo_CC_direct : tgo_CC_ewald)(&S.p, L.data(), nd.x, ym.data(), yx.data(), (int)lst.size());
+                        w = lst.size();
+                    } else {
+                        gather_parts(S, lst, y);
+                        if (use_ref == 1)
+                            (kind == TGO_CP_D ? S.ref_cp_d : S.ref_cp_e)(&S.p, L.data(), nd.x, y.data(), (int)(y.size() / 3));
+                        else
+                            (kind == TGO_CP_D ? tgo_CP_direct : tgo_CP_ewald)(&S.p, L.data(), nd.x, y.data(), (int)(y.size() / 3));
+                        w = y.size() / 3;
+                    }
+                } else {
+                    f.assign(4 * (size_t)nx, 0.0);
+                    if (kind == TGO_PC_D || kind == TGO_PC_E) {
+                        gather_multi(S, lst, ym, yx);
+                        if (use_ref == 1)
+                            (kind == TGO_PC_D ? S.ref_pc_d : S.ref_pc_e)(&S.p, f.data(), xs, nx, ym.data(), yx.data(), (int)lst.size());
+                        else
+                            (kind == TGO_PC_D ? tgo_PC_direct : tgo_PC_ewald)(&S.p, f.data(), xs, nx, ym.data(), yx.data(), (int)lst.size());
+                        w = (uint64_t)nx * lst.size();
+                    } else {
+                        gather_parts(S, lst, y);
+                        if (use_ref == 1)
+                            (kind == TGO_PP_D ? S.ref_pp_d : S.ref_pp_e)(&S.p, f.data(), xs, nx, y.data(), (int)(y.size() / 3), 1);
+                        else
+                            (kind == TGO_PP_D ? tgo_PP_direct : tgo_PP_ewald)(&S.p, f.data(), xs, nx, y.data(), (int)(y.size() / 3), 1);
+                        w = (uint64_t)nx * (y.size() / 3);
+                    }
+                }
+                work.fetch_add(w);
+                const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (el > budget_s) stop.store(true);
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; t++) th.emplace_back(body);
+        for (auto &t : th) t.join();
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        done[kind] = work.load();
+        ns_per[kind] = done[kind] ? el * 1e9 / (double)done[kind] : 0.0;
+    }
     return 0;
 }
 

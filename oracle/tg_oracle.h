@@ -119,6 +119,9 @@ int tgo_get_expansions(void *h, double *L);
  * [PP_d, PP_e, CC_d, CC_e, CP_d, CP_e] plus clean counts
  * [pairs PP_d, PP_e, PC_d, PC_e, CC_d, CC_e, CP_d, CP_e] and flops (reference convention) */
 int tgo_get_stats(void *h, uint64_t ref_stats[6], uint64_t counts[8], uint64_t *flops);
+/* host throughput of each interaction kind (ns per interaction, list-kind
+ * order), sampled over random sinks for at most budget_s seconds per kind */
+int tgo_kind_costs(void *h, int use_ref, int nthreads, double budget_s, uint64_t seed, double *ns_per, uint64_t *done);
 
 /* kick/drift (clean KDK restatement of src/part_vect.cpp:341-436, 493-540) */
 int tgo_kick(void *h, double dt);                 /* v += g * G * dt  (float v, double math) */

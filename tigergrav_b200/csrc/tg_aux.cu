@@ -54,7 +54,7 @@ static std::vector<std::array<int, 3>> lattice(int n2max) {
 }
 
 /* periodic_parts (tigergrav/green.hpp:30-59) in FP64: one thread per h */
-__global__ void k_periodic_parts(const float4 *four, int nf, double *Hd, float *Hf) {
+__global__ void k_periodic_parts(const float4 *four, int nf, double scale, double *Hd, float *Hf) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nf) return;
     const float4 hv = four[t];
@@ -92,8 +92,8 @@ __global__ void k_periodic_parts(const float4 *four, int nf, double *Hd, float *
         }
     }
     for (int i = 0; i < LP; i++) {
-        Hd[LP * t + i] = D[i];
-        Hf[LP * t + i] = F[i];
+        Hd[LP * t + i] = scale * D[i];
+        Hf[LP * t + i] = (float)scale * F[i]; /* scale is a power of two: exact */
     }
 }
 
@@ -101,20 +101,26 @@ int ewald_tables(Solver &S, cudaStream_t st) {
     if (S.have_tables) return TG_OK;
     const auto real = lattice(17), four = lattice(9);
     if ((int)real.size() != NREAL || (int)four.size() != NFOUR) return TG_ERR_STATE;
-    std::vector<float4> r4(NREAL), f4(NFOUR);
+    std::vector<float4> r4(NREAL), f4;
     /* device order: increasing |n|^2, so the first NREAL_F32 are the candidates of the FP32 cut */
     for (int i = 0; i < NREAL; i++) {
         const auto &v = real[NREAL - 1 - i];
         r4[i] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
     }
-    for (int i = 0; i < NFOUR; i++) f4[i] = make_float4((float)four[i][0], (float)four[i][1], (float)four[i][2], 0.0f);
+    /* one h of each pair +-h: first non-zero component positive; its coefficients doubled */
+    for (int i = 0; i < NFOUR; i++) {
+        const auto &v = four[i];
+        const int lead = v[0] != 0 ? v[0] : (v[1] != 0 ? v[1] : v[2]);
+        if (lead > 0) f4.push_back(make_float4((float)v[0], (float)v[1], (float)v[2], 0.0f));
+    }
+    if ((int)f4.size() != NFOUR_HALF) return TG_ERR_STATE;
     TG_TRY(ensure(S.ew_real, NREAL));
-    TG_TRY(ensure(S.ew_four, NFOUR));
-    TG_TRY(ensure(S.ew_Hf, NFOUR * LP));
-    TG_TRY(ensure(S.ew_Hd, NFOUR * LP));
+    TG_TRY(ensure(S.ew_four, NFOUR_HALF));
+    TG_TRY(ensure(S.ew_Hf, NFOUR_HALF * LP));
+    TG_TRY(ensure(S.ew_Hd, NFOUR_HALF * LP));
     TG_CUDA(cudaMemcpyAsync(S.ew_real.p, r4.data(), sizeof(float4) * NREAL, cudaMemcpyHostToDevice, st));
-    TG_CUDA(cudaMemcpyAsync(S.ew_four.p, f4.data(), sizeof(float4) * NFOUR, cudaMemcpyHostToDevice, st));
-    k_periodic_parts<<<(NFOUR + 63) / 64, 64, 0, st>>>(S.ew_four.p, NFOUR, S.ew_Hd.p, S.ew_Hf.p);
+    TG_CUDA(cudaMemcpyAsync(S.ew_four.p, f4.data(), sizeof(float4) * NFOUR_HALF, cudaMemcpyHostToDevice, st));
+    k_periodic_parts<<<(NFOUR_HALF + 63) / 64, 64, 0, st>>>(S.ew_four.p, NFOUR_HALF, 2.0, S.ew_Hd.p, S.ew_Hf.p);
     TG_TRY(launched(S));
     TG_CUDA(cudaStreamSynchronize(st)); /* host vectors go out of scope */
     S.have_tables = true;

@@ -23,6 +23,7 @@ constexpr double POS_INV = 1.0 / 4294967296.0;
 constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
 constexpr int NREAL_F32 = 179; /* |n|^2 <= 12: every n that can lie within the FP32 cut 2.6 of |X| <= sqrt(3)/2 */
 constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
+constexpr int NFOUR_HALF = 61; /* one of each pair +-h (h != 0) */
 constexpr float EWALD_RCUT = 1.0e-6f;
 constexpr float EWALD_PHI0 = 2.8372975f; /* r -> 0 limit (tigergrav/green.hpp:272) */
 
@@ -114,8 +115,6 @@ __device__ __forceinline__ float t_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double t_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float t_rcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double t_rcp(double x) { return 1.0 / x; }
-__device__ __forceinline__ void t_sincospi(float x, float *s, float *c) { sincospif(x, s, c); }
-__device__ __forceinline__ void t_sincospi(double x, double *s, double *c) { sincospi(x, s, c); }
 
 /* erfc(x) and exp(-x^2).  FP32: the Abramowitz & Stegun 7.1.26 rational
  * approximation that the reference uses (tigergrav/simd.hpp:676-692), with
@@ -228,9 +227,9 @@ __device__ __forceinline__ void green_direct(const T *dX, T *D) {
 /* Ewald tables (tigergrav/green.hpp:8-59), generated in FP64 on the device. */
 struct EwaldTables {
     const float4 *real; /* NREAL lattice vectors n by increasing |n|^2 (w = |n|^2) */
-    const float4 *four; /* NFOUR reciprocal vectors h (w unused) */
-    const float *Hf;    /* NFOUR x 35 periodic_parts coefficients, float */
-    const double *Hd;   /* NFOUR x 35, double */
+    const float4 *four; /* NFOUR_HALF reciprocal vectors h, first non-zero component > 0 (w unused) */
+    const float *Hf;    /* NFOUR_HALF x 35: 2 x periodic_parts coefficients, float */
+    const double *Hd;   /* NFOUR_HALF x 35, double */
 };
 
 /* Real-space cut of the Ewald sum.  The reference masks images at r >= 3.6
@@ -243,10 +242,33 @@ template <class T> __device__ __forceinline__ T ewald_rcut2();
 template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 6.76f; }
 template <> __device__ __forceinline__ double ewald_rcut2<double>() { return 12.96; }
 
-/* One real-space image of green_ewald (tigergrav/green.hpp:212-236), alpha = 2,
- * at separation dx (|dx|^2 = r2 inside the cut). */
-template <class T, class A>
-__device__ __forceinline__ void ewald_real_image(A *D, const T *dx, T r2) {
+/* Sums over the real-space images that green_ewald's derivative tensors are
+ * built from (tigergrav/green.hpp:62-117 applied per image, 212-236): with
+ * radial factors d0..d4 of each image at separation x,
+ *   D0 = S d0,  D_a = S d1 x_a,  D_ab = S d2 x_a x_b + delta_ab S d1,
+ *   D_abc = S d3 x_a x_b x_c + (delta_ab S d2 x_c + 2 perms),
+ *   D_abcd = S d4 x_a x_b x_c x_d + (delta_ab S d3 x_c x_d + 5 perms)
+ *            + (delta_ab delta_cd + 2 perms) S d2.
+ * The pure products accumulate straight into D; the four delta sums below
+ * are folded in once per evaluation by ewald_mom_finish -- the same tensor as
+ * adding each image's full derivative set, at half the work per image. */
+template <class T> struct EwaldMom {
+    T s3[6]; /* S d3 x_a x_b, slot I2(a, b) */
+    T t2[3]; /* S d2 x_a */
+    T u1;    /* S d1 */
+    T s2;    /* S d2 */
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int k = 0; k < 6; k++) s3[k] = T(0);
+        t2[0] = t2[1] = t2[2] = T(0);
+        u1 = s2 = T(0);
+    }
+};
+
+/* One real-space image (tigergrav/green.hpp:212-236), alpha = 2, at
+ * separation dx with |dx|^2 = r2 inside the cut. */
+template <class T>
+__device__ __forceinline__ void ewald_real_image(T *D, EwaldMom<T> &m, const T *dx, T r2) {
     const T rinv = t_rsqrt(r2);
     const T r = r2 * rinv;
     const T r2inv = rinv * rinv;
@@ -263,60 +285,152 @@ __device__ __forceinline__ void ewald_real_image(A *D, const T *dx, T r2) {
     const T d2 = -fma(expfactor, fma(T(8), r2, T(3)), T(3) * erfc) * r5inv;
     const T d3 = fma(expfactor, (T(15) + fma(T(40), r2, T(64) * r4)), T(15) * erfc) * r7inv;
     const T d4 = -fma(expfactor, fma(T(8) * r2, (T(35) + fma(T(56), r2, T(64) * r4)), T(105)), T(105) * erfc) * r9inv;
-    green_deriv_add<T, A>(D, d0, d1, d2, d3, d4, dx);
-}
-
-/* Visit the lattice images n of the reference's set (|n|^2 <= 17,
- * tigergrav/green.hpp:3,8-28) with |X - n|^2 < ewald_rcut2, walking the
- * integer ranges that the cut allows instead of testing all 305 vectors.
- * fn(dx, r2, is_origin) is called once per image.  Caller guarantees
- * |X| > 1e-6 (the reference's zmask = 1). */
-template <class T, class F>
-__device__ __forceinline__ void ewald_images(const T *X, F &&fn) {
-    const T R2 = ewald_rcut2<T>();
-    const T R = t_sqrt(R2);
-    const int nx0 = (int)ceil(X[0] - R), nx1 = (int)floor(X[0] + R);
-    for (int nx = nx0; nx <= nx1; nx++) {
-        const T dx = X[0] - T(nx);
-        const T rx = R2 - dx * dx;
-        if (!(rx > T(0))) continue;
-        const T ry = t_sqrt(rx);
-        const int ny0 = (int)ceil(X[1] - ry), ny1 = (int)floor(X[1] + ry);
-        for (int ny = ny0; ny <= ny1; ny++) {
-            const T dy = X[1] - T(ny);
-            const T rxy = rx - dy * dy;
-            if (!(rxy > T(0))) continue;
-            const T rz = t_sqrt(rxy);
-            const int nz0 = (int)ceil(X[2] - rz), nz1 = (int)floor(X[2] + rz);
-            for (int nz = nz0; nz <= nz1; nz++) {
-                if (nx * nx + ny * ny + nz * nz > 17) continue;
-                const T d[3] = {dx, dy, X[2] - T(nz)};
-                const T r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-                if (!(r2 < R2)) continue;
-                fn(d, r2, nx == 0 && ny == 0 && nz == 0);
+    D[E0()] += d0;
+    m.u1 += d1;
+    m.s2 += d2;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E1(a)] = fma(d1, dx[a], D[E1(a)]);
+        m.t2[a] = fma(d2, dx[a], m.t2[a]);
+        const T d2a = d2 * dx[a], d3a = d3 * dx[a], d4a = d4 * dx[a];
+#pragma unroll
+        for (int b = a; b < 3; b++) {
+            D[E2(a, b)] = fma(d2a, dx[b], D[E2(a, b)]);
+            m.s3[I2(a, b)] = fma(d3a, dx[b], m.s3[I2(a, b)]);
+            const T d3ab = d3a * dx[b], d4ab = d4a * dx[b];
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                D[E3(a, b, c)] = fma(d3ab, dx[c], D[E3(a, b, c)]);
+                const T d4abc = d4ab * dx[c];
+#pragma unroll
+                for (int d = c; d < 3; d++) D[E4(a, b, c, d)] = fma(d4abc, dx[d], D[E4(a, b, c, d)]);
             }
         }
     }
 }
 
-/* One reciprocal-space term of green_ewald (tigergrav/green.hpp:237-264). */
-template <class T, class A>
-__device__ __forceinline__ void ewald_four_term(A *D, const T *X, float4 h, const T *H) {
-    const T hdotdx = X[0] * T(h.x) + X[1] * T(h.y) + X[2] * T(h.z);
-    T si, co;
-    t_sincospi(T(2) * hdotdx, &si, &co);
-    D[E0()] += H[E0()] * co;
+/* fold the delta terms of the image sums into D (once per evaluation) */
+template <class T>
+__device__ __forceinline__ void ewald_mom_finish(T *D, const EwaldMom<T> &m) {
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        D[E1(a)] += H[E1(a)] * si;
+        D[E2(a, a)] += m.u1;
+#pragma unroll
+        for (int b = a; b < 3; b++)
+#pragma unroll
+            for (int c = b; c < 3; c++) {
+                T v = T(0);
+                if (a == b) v += m.t2[c];
+                if (a == c) v += m.t2[b];
+                if (b == c) v += m.t2[a];
+                D[E3(a, b, c)] += v;
+#pragma unroll
+                for (int d = c; d < 3; d++) {
+                    T w = T(0);
+                    if (a == b) w += m.s3[I2(c, d)];
+                    if (a == c) w += m.s3[I2(b, d)];
+                    if (a == d) w += m.s3[I2(b, c)];
+                    if (b == c) w += m.s3[I2(a, d)];
+                    if (b == d) w += m.s3[I2(a, c)];
+                    if (c == d) w += m.s3[I2(a, b)];
+                    const int pairs = (a == b && c == d) + (a == c && b == d) + (a == d && b == c);
+                    D[E4(a, b, c, d)] += w + T(pairs) * m.s2;
+                }
+            }
+    }
+}
+
+/* Visit the lattice images n of the reference's set (|n|^2 <= 17,
+ * tigergrav/green.hpp:3,8-28) with |X - n|^2 < ewald_rcut2, walking the
+ * integer ranges that the cut allows instead of testing all 305 vectors.
+ * The three nested ranges are flattened into one loop that advances each
+ * lane to its next image, so a warp whose lanes hold different X runs the
+ * image body together (about 75 images per lane, in lockstep) instead of
+ * diverging at every level of the nest.  fn(dx, r2, is_origin) is called
+ * once per image.  Caller guarantees |X| > 1e-6 (the reference's zmask = 1). */
+template <class T, class F>
+__device__ __forceinline__ void ewald_images(const T *X, F &&fn) {
+    const T R2 = ewald_rcut2<T>();
+    const T R = t_sqrt(R2);
+    int nx = (int)ceil(X[0] - R) - 1;
+    const int nx1 = (int)floor(X[0] + R);
+    int ny = 0, ny1 = -1, nz = 0, nz1 = -1;
+    T dx = T(0), dy = T(0), rx = T(0);
+    for (;;) {
+        /* advance to the next (nx, ny, nz) inside the cut; columns and rows
+         * that the cut leaves empty are skipped here */
+        nz++;
+        bool done = false;
+        while (nz > nz1) {
+            ny++;
+            while (ny > ny1) {
+                nx++;
+                if (nx > nx1) {
+                    done = true;
+                    break;
+                }
+                dx = X[0] - T(nx);
+                rx = R2 - dx * dx;
+                if (rx > T(0)) {
+                    const T ry = t_sqrt(rx);
+                    ny = (int)ceil(X[1] - ry);
+                    ny1 = (int)floor(X[1] + ry);
+                } else {
+                    ny = 1;
+                    ny1 = 0;
+                }
+            }
+            if (done) break;
+            dy = X[1] - T(ny);
+            const T rxy = rx - dy * dy;
+            if (rxy > T(0)) {
+                const T rz = t_sqrt(rxy);
+                nz = (int)ceil(X[2] - rz);
+                nz1 = (int)floor(X[2] + rz);
+            } else {
+                nz = 1;
+                nz1 = 0;
+            }
+        }
+        if (done) break;
+        if (nx * nx + ny * ny + nz * nz > 17) continue;
+        const T d[3] = {dx, dy, X[2] - T(nz)};
+        const T r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        if (!(r2 < R2)) continue;
+        fn(d, r2, nx == 0 && ny == 0 && nz == 0);
+    }
+}
+
+/* sin and cos of 2 pi x.  FP32: exact reduction to r = x - rint(x) in
+ * [-1/2, 1/2], then the hardware sin/cos of 2 pi r (|2 pi r| <= pi, absolute
+ * error ~4e-7, below the rounding of h.X itself); FP64: sincospi. */
+__device__ __forceinline__ void t_sincos2pi(float x, float *s, float *c) {
+    const float r = x - rintf(x);
+    __sincosf(6.2831853071795865f * r, s, c);
+}
+__device__ __forceinline__ void t_sincos2pi(double x, double *s, double *c) { sincospi(2.0 * x, s, c); }
+
+/* The reciprocal-space sum of green_ewald (tigergrav/green.hpp:237-264) over
+ * the 61 vectors h with first non-zero component > 0: the terms of h and -h
+ * are equal (H(h) is even/odd in h like cos/sin), so the table holds 2 H(h)
+ * and each pair costs one term; h = 0 has H = 0. */
+template <class T>
+__device__ __forceinline__ void ewald_four_term(T *D, const T *X, float4 h, const T *H) {
+    const T hdotdx = X[0] * T(h.x) + X[1] * T(h.y) + X[2] * T(h.z);
+    T si, co;
+    t_sincos2pi(hdotdx, &si, &co);
+    D[E0()] = fma(H[E0()], co, D[E0()]);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        D[E1(a)] = fma(H[E1(a)], si, D[E1(a)]);
 #pragma unroll
         for (int b = 0; b <= a; b++) {
-            D[E2(a, b)] += H[E2(a, b)] * co;
+            D[E2(a, b)] = fma(H[E2(a, b)], co, D[E2(a, b)]);
 #pragma unroll
             for (int c = 0; c <= b; c++) {
-                D[E3(a, b, c)] += H[E3(a, b, c)] * si;
+                D[E3(a, b, c)] = fma(H[E3(a, b, c)], si, D[E3(a, b, c)]);
 #pragma unroll
-                for (int d = 0; d <= c; d++) D[E4(a, b, c, d)] += H[E4(a, b, c, d)] * co;
+                for (int d = 0; d <= c; d++) D[E4(a, b, c, d)] = fma(H[E4(a, b, c, d)], co, D[E4(a, b, c, d)]);
             }
         }
     }

@@ -1,0 +1,128 @@
+/*
+ * tg_ewald_leaf.cuh -- the leaf-sink Ewald kernels (gravity_PC_ewald,
+ * src/gravity.cpp:616-678; gravity_PP_ewald, :491-614) as balanced work
+ * units.  Included by tg_gravity.cu.
+ *
+ * The Ewald lists of a leaf are very uneven: large leaves in voids fail the
+ * Ewald self test and interact with every leaf within (r_a + r_b)/theta, so
+ * at theta = 0.2 on a clustered box 1% of the leaves hold half the PP_Ewald
+ * pairs (up to 9e6 for one leaf).  One block per leaf would leave a tail of a
+ * few blocks running for most of the kernel.  Instead each leaf's PP_E list
+ * is cut into chunks of EW_KPP source leaves and its PC_E list into chunks of
+ * EW_KPC source nodes; one 64-thread block (a thread per sink) evaluates one
+ * chunk and writes its sinks' partial sums to its own slot of a scratch
+ * array; k_ewald_reduce then adds a leaf's chunk sums in chunk order to the
+ * leaf's FP64 accumulators.  The result does not depend on scheduling.
+ */
+#pragma once
+
+constexpr int EW_KPP = 32;  /* PP_E source leaves per chunk (<= 32 * 64 * 64 pairs) */
+constexpr int EW_KPC = 128; /* PC_E source nodes per chunk */
+
+/* chunks per leaf; cnt[nleaves] = 0 so that an exclusive scan ends in the total */
+__global__ void k_ewald_count(const int32_t *__restrict__ leaves, int32_t nleaves, ListView LV,
+                              int32_t *__restrict__ cnt) {
+    const int32_t li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li > nleaves) return;
+    if (li == nleaves) {
+        cnt[li] = 0;
+        return;
+    }
+    const int32_t leaf = leaves[li];
+    const int32_t npp = LV.len[TG_PP_E][leaf], npc = LV.len[TG_PC_E][leaf];
+    cnt[li] = (npp + EW_KPP - 1) / EW_KPP + (npc + EW_KPC - 1) / EW_KPC;
+}
+
+/* one chunk: PP_E entries [k EW_KPP, ...) or PC_E entries [(k - npp) EW_KPC, ...) of its leaf */
+template <class T>
+__global__ void __launch_bounds__(64) k_ewald_chunk(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
+                                                    const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
+                                                    const int32_t *__restrict__ pe, const MSrc *__restrict__ ms,
+                                                    const int4 *__restrict__ pos, ListView LV, EwaldTables E,
+                                                    double *__restrict__ part) {
+    __shared__ int4 sy[64];
+    const int tid = threadIdx.x;
+    const int64_t c = blockIdx.x;
+    int32_t lo = 0, hi = nleaves - 1; /* the leaf: largest li with off[li] <= c */
+    while (lo < hi) {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if ((int64_t)off[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    const int32_t li = lo, k = (int32_t)(c - off[li]);
+    const int32_t leaf = leaves[li];
+    const int32_t b = pb[leaf], cnt = pe[leaf] - b;
+    const bool active = tid < cnt;
+    const int4 xi4 = pos[b + (active ? tid : 0)];
+    const int32_t xi[3] = {xi4.x, xi4.y, xi4.z};
+    Acc<T> aphi, ag[3];
+    aphi.init(0.0);
+    for (int d = 0; d < 3; d++) ag[d].init(0.0);
+    const int32_t lpp = LV.len[TG_PP_E][leaf];
+    const int32_t npp = (lpp + EW_KPP - 1) / EW_KPP;
+    if (k < npp) {
+        const int32_t *lst = LV.pool[TG_PP_E] + LV.off[TG_PP_E][leaf];
+        const int32_t e1 = min(lpp, (k + 1) * EW_KPP);
+        const T m = T(P.m_d);
+        for (int32_t e = k * EW_KPP; e < e1; e++) {
+            const int32_t src = lst[e];
+            const int32_t sb = pb[src], sn = pe[src] - sb;
+            for (int32_t base = 0; base < sn; base += 64) {
+                const int32_t nt = min(64, sn - base);
+                __syncthreads();
+                if (tid < nt) sy[tid] = pos[sb + base + tid];
+                __syncthreads();
+                for (int32_t q = 0; q < nt; q++) {
+                    const int4 y = sy[q];
+                    T dX[3] = {wrap_sep_t<T>(xi[0], y.x), wrap_sep_t<T>(xi[1], y.y), wrap_sep_t<T>(xi[2], y.z)};
+                    T ph, g[3];
+                    pp_ewald_pair<T>(E, dX, ph, g);
+                    aphi.add(m * ph);
+                    for (int d = 0; d < 3; d++) ag[d].add(m * g[d]);
+                }
+            }
+        }
+    } else {
+        const int32_t lpc = LV.len[TG_PC_E][leaf];
+        const int32_t *lst = LV.pool[TG_PC_E] + LV.off[TG_PC_E][leaf];
+        const int32_t e0 = (k - npp) * EW_KPC, e1 = min(lpc, e0 + EW_KPC);
+        for (int32_t e = e0; e < e1; e++) {
+            const MSrc &s = ms[lst[e]];
+            T dX[3], D[LP], M[MP];
+#pragma unroll
+            for (int d = 0; d < 3; d++) dX[d] = sep<T>(xi[d], s.x[d], true);
+#pragma unroll
+            for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
+            green_ewald_full<T>(E, dX, D);
+            T ph, g[3];
+            contract_M2P<T>(ph, g, M, D);
+            aphi.add(ph);
+            for (int d = 0; d < 3; d++) ag[d].add(g[d]);
+        }
+    }
+    if (active) {
+        double *o = part + 4 * (c * 64 + tid);
+        o[0] = aphi.get();
+        for (int d = 0; d < 3; d++) o[1 + d] = ag[d].get();
+    }
+}
+
+/* add each leaf's chunk sums, in chunk order, to its FP64 accumulators */
+__global__ void __launch_bounds__(64) k_ewald_reduce(const int32_t *__restrict__ leaves, int32_t nleaves,
+                                                     const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
+                                                     const int32_t *__restrict__ pe, const double *__restrict__ part,
+                                                     double *__restrict__ acc) {
+    const int32_t li = blockIdx.x;
+    const int tid = threadIdx.x;
+    if (li >= nleaves) return;
+    const int32_t leaf = leaves[li];
+    const int32_t b = pb[leaf], cnt = pe[leaf] - b;
+    if (tid >= cnt || off[li + 1] == off[li]) return;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t c = off[li]; c < off[li + 1]; c++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[q] += part[4 * (c * 64 + tid) + q];
+    double *o = acc + 4 * (int64_t)(b + tid);
+#pragma unroll
+    for (int q = 0; q < 4; q++) o[q] += v[q];
+}

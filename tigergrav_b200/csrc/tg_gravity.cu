@@ -165,11 +165,11 @@ __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0
         gy -= dy * d1;
         gz -= dz * d1;
     });
-    for (int t = 0; t < NFOUR; t++) {
+    for (int t = 0; t < NFOUR_HALF; t++) {
         const float4 h = __ldg(&E.four[t]);
         const T hdotdx = dX0[0] * T(h.x) + dX0[1] * T(h.y) + dX0[2] * T(h.z);
         T s, c;
-        t_sincospi(T(2) * hdotdx, &s, &c);
+        t_sincos2pi(hdotdx, &s, &c);
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
         ph += H[E0()] * c;
         gx -= H[E1(0)] * s;
@@ -195,10 +195,13 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
         D[0] = T(EWALD_PHI0);
         return;
     }
-    ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T, T>(D, d, rr2); });
-    for (int t = 0; t < NFOUR; t++) {
+    EwaldMom<T> mom;
+    mom.init();
+    ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T>(D, mom, d, rr2); });
+    ewald_mom_finish<T>(D, mom);
+    for (int t = 0; t < NFOUR_HALF; t++) {
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
-        ewald_four_term<T, T>(D, X, __ldg(&E.four[t]), H);
+        ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
     ewald_finish<T, T>(D, X);
 }
@@ -213,15 +216,18 @@ __device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *
 #pragma unroll
     for (int k = 0; k < LP; k++) D[k] = T(0);
     const int ncand = sizeof(T) == 4 ? NREAL_F32 : NREAL;
+    EwaldMom<T> mom;
+    mom.init();
     for (int t = lane; t < ncand; t += 32) {
         const float4 n = __ldg(&E.real[t]);
         const T dx[3] = {X[0] - T(n.x), X[1] - T(n.y), X[2] - T(n.z)};
         const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
-        if (r2 < ewald_rcut2<T>()) ewald_real_image<T, T>(D, dx, r2);
+        if (r2 < ewald_rcut2<T>() && n.w <= 17.0f) ewald_real_image<T>(D, mom, dx, r2);
     }
-    for (int t = lane; t < NFOUR; t += 32) {
+    ewald_mom_finish<T>(D, mom);
+    for (int t = lane; t < NFOUR_HALF; t += 32) {
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
-        ewald_four_term<T, T>(D, X, __ldg(&E.four[t]), H);
+        ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
     if (lane == 0) ewald_finish<T, T>(D, X);
 }
@@ -374,7 +380,7 @@ __global__ void k_l2l(int64_t first, int64_t count, const int32_t *__restrict__ 
 }
 
 /* ---- leaf kernel ---- */
-template <class T, int BLOCK, bool PP = true>
+template <class T, int BLOCK, bool PP = true, bool EW = true>
 __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
                                                 const int32_t *__restrict__ pb, const int32_t *__restrict__ pe,
                                                 const MSrc *__restrict__ ms, const int4 *__restrict__ pos, ListView LV,
@@ -456,7 +462,7 @@ __global__ void __launch_bounds__(BLOCK) k_leaf(GParams P, const int32_t *__rest
                 }
             }
         }
-        if (per) {
+        if (EW && per) {
             /* PC Ewald (src/gravity.cpp:616-678) */
             const int32_t *lst = LV.pool[TG_PC_E] + LV.off[TG_PC_E][leaf];
             const int32_t len = LV.len[TG_PC_E][leaf];
@@ -542,6 +548,7 @@ __device__ __forceinline__ int32_t rel_off(int32_t Y, int32_t Xr, bool per, uint
 }
 
 #include "tg_pp.cuh"
+#include "tg_ewald_leaf.cuh"
 
 /* ---------------- kernel-level seams ---------------- */
 
@@ -651,6 +658,36 @@ static ListView listview(Solver &S) {
     return LV;
 }
 
+/* the leaf Ewald lists (PP_E, PC_E) of every leaf, in balanced chunks, added
+ * to the FP64 accumulators accd (leaf_max <= 64) */
+static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const EwaldTables &E, bool f64,
+                      cudaStream_t st) {
+    const int32_t nleaves = (int32_t)S.st.leaves;
+    TG_TRY(ensure(S.ew_cnt, (size_t)nleaves + 1));
+    TG_TRY(ensure(S.ew_off, (size_t)nleaves + 1));
+    k_ewald_count<<<(nleaves + 1 + 127) / 128, 128, 0, st>>>(S.idx.p, nleaves, LV, S.ew_cnt.p);
+    TG_TRY(launched(S));
+    size_t stmp = 0;
+    TG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, stmp, S.ew_cnt.p, S.ew_off.p, nleaves + 1, st));
+    TG_TRY(ensure(S.cub_tmp, stmp));
+    TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, stmp, S.ew_cnt.p, S.ew_off.p, nleaves + 1, st));
+    int32_t total = 0;
+    TG_CUDA(cudaMemcpyAsync(&total, S.ew_off.p + nleaves, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (total <= 0) return TG_OK;
+    TG_TRY(ensure(S.ew_part, (size_t)total * 64 * 4));
+    if (f64)
+        k_ewald_chunk<double><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
+                                                    S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p);
+    else
+        k_ewald_chunk<float><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
+                                                   S.pos.p, LV, E, S.ew_part.p);
+    TG_TRY(launched(S));
+    k_ewald_reduce<<<nleaves, 64, 0, st>>>(S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.ew_part.p, S.accd.p);
+    TG_TRY(launched(S));
+    return TG_OK;
+}
+
 int gravity_forces(Solver &S, cudaStream_t st) {
     if (!S.have_lists) return TG_ERR_STATE;
     TG_TRY(ewald_tables(S, st));
@@ -688,14 +725,17 @@ int gravity_forces(Solver &S, cudaStream_t st) {
     if (nleaves > 0) {
         const int g = nleaves;
         if (S.prm.leaf_max <= 64) {
+            /* L2P, PC direct (and for FP64 PP direct) per leaf; the Ewald lists as balanced chunks */
             if (f64)
-                k_leaf<double, 64><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV, E,
-                                                     S.nd_L.p, nullptr, S.accd.p);
-            else {
-                /* far part in FP64, then PP direct over the same leaves */
-                k_leaf<float, 64, false><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
-                                                           S.pos.p, LV, E, S.nd_L.p, nullptr, S.accd.p);
-                TG_TRY(launched(S));
+                k_leaf<double, 64, true, false><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
+                                                                  S.pos.p, LV, E, S.nd_L.p, nullptr, S.accd.p);
+            else
+                k_leaf<float, 64, false, false><<<g, 64, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p,
+                                                                  S.nd_ms.p, S.pos.p, LV, E, S.nd_L.p, nullptr,
+                                                                  S.accd.p);
+            TG_TRY(launched(S));
+            if (S.prm.ewald) TG_TRY(leaf_ewald(S, P, LV, E, f64, st));
+            if (!f64) {
                 if (S.have_events) {
                     TG_CUDA(cudaEventRecord(S.ev[6], st));
                     S.pp_timed = true;

@@ -110,6 +110,8 @@ struct Solver {
     size_t h_stage_bytes = 0;
 
     /* Ewald tables */
+    DevBuf<int32_t> ew_cnt, ew_off; /* leaf Ewald chunks per leaf, and their exclusive scan */
+    DevBuf<double> ew_part;          /* 64 x 4 partial sums per chunk */
     DevBuf<float4> ew_real, ew_four;
     DevBuf<float> ew_Hf;
     DevBuf<double> ew_Hd;

@@ -57,7 +57,7 @@ def clustered(nside: int, seed: int = 2, rms: float = 0.5) -> np.ndarray:
     amp[0, 0, 0] = 0.0
     psi = np.empty((3, nside, nside, nside), np.float64)
     for d, kd in enumerate((kx, ky, kzz)):
-        psi[d] = np.fft.irfftn(1j * kd * amp, s=(nside, nside, nside))
+        psi[d] = np.fft.irfftn(1j * kd * amp, s=(nside, nside, nside), axes=(0, 1, 2))
     del amp, W
     cur = np.sqrt(np.mean(np.sum(psi * psi, axis=0)))
     psi *= (rms / nside) / cur
