@@ -64,13 +64,13 @@ PP_FLOPS = 26
 # FP32 operations per interaction of the Ewald and multipole kernels, counted
 # from the source the same way.  One real-space image: separation and r^2 8,
 # rsqrt and powers of 1/r 8, erfc/exp 18, d0..d4 31, the moment sums 120 ->
-# 185; 73.6 images on average inside the FP32 cut r < 2.6 (4/3 pi 2.6^3).
+# 185; 44.6 images on average inside the FP32 cut r < 2.2 (4/3 pi 2.2^3).
 # One reciprocal term of the half sum: h.X 5, reduction and sin/cos 5, 35
-# FMAs 70 -> 80; 61 terms.  Finish 105.  green_ewald = 18.6k.  Contractions:
+# FMAs 70 -> 80; 61 terms.  Finish 105.  green_ewald = 13.2k.  Contractions:
 # M2L 858, M2P 414, P2L 70 (direct kernels: the reference's constants).
-# PP_E pair: 72.6 images x 44 + 61 x 18 + 30 = 4.3k.
-NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 19500, "CP_E": 18700}
-LEAF_FLOPS = {"PC_D": 581, "PC_E": 19000, "PP_E": 4300}
+# PP_E pair: 43.6 images x 44 + 61 x 18 + 30 = 3.0k.
+NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 14100, "CP_E": 13300}
+LEAF_FLOPS = {"PC_D": 581, "PC_E": 13600, "PP_E": 3000}
 
 
 def make_particles(w):

@@ -21,7 +21,7 @@ constexpr int LP = 35;
 constexpr double POS_MAX = 4294967296.0;
 constexpr double POS_INV = 1.0 / 4294967296.0;
 constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
-constexpr int NREAL_F32 = 179; /* |n|^2 <= 12: every n that can lie within the FP32 cut 2.6 of |X| <= sqrt(3)/2 */
+constexpr int NREAL_F32 = 123; /* |n|^2 <= 9: every n that can lie within the FP32 cut 2.2 of |X| <= sqrt(3)/2 */
 constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
 constexpr int NFOUR_HALF = 61; /* one of each pair +-h (h != 0) */
 constexpr float EWALD_RCUT = 1.0e-6f;
@@ -233,13 +233,14 @@ struct EwaldTables {
 };
 
 /* Real-space cut of the Ewald sum.  The reference masks images at r >= 3.6
- * (tigergrav/green.hpp:220); the FP64 path keeps that.  Images beyond
- * r = 2.6 add at most 1.4e-7 (erfc(5.2) ~ 1e-12 times the derivative
- * polynomials) to any r^k-scaled derivative -- below the FP32 rounding of the
- * sums and below the 1.5e-7 error of the reference's own A&S erfc -- so the
- * FP32 path stops there and evaluates ~80 images instead of ~200. */
+ * (tigergrav/green.hpp:220); the FP64 path keeps that.  An image at r >= 2.2
+ * adds at most 1.1e-6 to the fourth derivative and 1e-8 to the potential
+ * and force factors (erfc(4.4) = 3e-10; exp(-19.4) times the derivative
+ * polynomials), i.e. below 1e-7 of each derivative of green_ewald and below
+ * the error of the reference's own A&S erfc (1.5e-7); the FP32 path stops
+ * there and evaluates ~45 images instead of ~200. */
 template <class T> __device__ __forceinline__ T ewald_rcut2();
-template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 6.76f; }
+template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 4.84f; }
 template <> __device__ __forceinline__ double ewald_rcut2<double>() { return 12.96; }
 
 /* Sums over the real-space images that green_ewald's derivative tensors are
@@ -345,7 +346,7 @@ __device__ __forceinline__ void ewald_mom_finish(T *D, const EwaldMom<T> &m) {
  * integer ranges that the cut allows instead of testing all 305 vectors.
  * The three nested ranges are flattened into one loop that advances each
  * lane to its next image, so a warp whose lanes hold different X runs the
- * image body together (about 75 images per lane, in lockstep) instead of
+ * image body together (about 45 images per lane in FP32, in lockstep) instead of
  * diverging at every level of the nest.  fn(dx, r2, is_origin) is called
  * once per image.  Caller guarantees |X| > 1e-6 (the reference's zmask = 1). */
 template <class T, class F>

@@ -18,6 +18,9 @@
 
 constexpr int EW_KPP = 32;  /* PP_E source leaves per chunk (<= 32 * 64 * 64 pairs) */
 constexpr int EW_KPC = 128; /* PC_E source nodes per chunk */
+#ifndef EW_MINB
+#define EW_MINB 12 /* resident 64-thread blocks per SM the kernel is compiled for */
+#endif
 
 /* chunks per leaf; cnt[nleaves] = 0 so that an exclusive scan ends in the total */
 __global__ void k_ewald_count(const int32_t *__restrict__ leaves, int32_t nleaves, ListView LV,
@@ -35,7 +38,7 @@ __global__ void k_ewald_count(const int32_t *__restrict__ leaves, int32_t nleave
 
 /* one chunk: PP_E entries [k EW_KPP, ...) or PC_E entries [(k - npp) EW_KPC, ...) of its leaf */
 template <class T>
-__global__ void __launch_bounds__(64) k_ewald_chunk(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
+__global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
                                                     const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
                                                     const int32_t *__restrict__ pe, const MSrc *__restrict__ ms,
                                                     const int4 *__restrict__ pos, ListView LV, EwaldTables E,

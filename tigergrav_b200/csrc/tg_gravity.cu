@@ -2,10 +2,12 @@
  * tg_gravity.cu -- the interaction kernels of kick_fmm (src/tree.cpp:400-631)
  * and the eight kernel-level seams of tigergrav/gravity.hpp:39-46.
  *
- *   k_node   one warp per node, lanes over sources: CC/CP direct and
- *            CC/CP Ewald (one thread evaluates a source's whole green_ewald,
- *            walking only the lattice images inside the real-space cut, then
- *            contracts it); lane sums are reduced in FP64 -> Lloc (35 doubles)
+ *   k_node   one warp per node, lanes over sources: CC/CP direct; lane
+ *            sums are reduced in FP64 -> Lloc (35 doubles)
+ *   k_node_ewald (tg_ewald_node.cuh)  CC/CP Ewald in balanced chunks, one
+ *            warp per chunk, one source's whole green_ewald per lane
+ *            (walking only the lattice images inside the real-space cut);
+ *            chunk sums added to Lloc in order
  *   k_l2l    one thread per node of a level, top-down:
  *            L = (L_parent << (x - x_parent)) + Lloc          (FP64)
  *   k_leaf   one block per leaf, one thread per sink particle: L2P, then
@@ -296,55 +298,6 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
                 }
             }
         }
-        if (per) {
-            /* CC Ewald (src/gravity.cpp:680-731) */
-            const int32_t *lst = LV.pool[TG_CC_E] + LV.off[TG_CC_E][i];
-            const int32_t len = LV.len[TG_CC_E][i];
-            if (len >= EWALD_WARP_LIST) {
-                for (int32_t j = lane; j < len; j += 32) {
-                    const MSrc &s = ms[lst[j]];
-                    T dX[3], D[LP], M[MP];
-#pragma unroll
-                    for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
-#pragma unroll
-                    for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-                    green_ewald_full<T>(E, dX, D);
-                    contract_M2L<T, T>(L, M, D);
-                }
-            } else {
-                for (int32_t j = 0; j < len; j++) {
-                    const MSrc &s = ms[lst[j]];
-                    T dX[3], D[LP], M[MP];
-#pragma unroll
-                    for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], s.x[d], true);
-                    if (!(dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2] > T(1.0e-12))) {
-                        /* the node itself: green_ewald(0) = phi0 only (tigergrav/green.hpp:279) */
-                        if (lane == 0) L[E0()] += T(s.m[0]) * T(EWALD_PHI0);
-                        continue;
-                    }
-#pragma unroll
-                    for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-                    green_ewald_warp<T>(E, dX, D, lane);
-                    contract_M2L<T, T>(L, M, D);
-                }
-            }
-            /* CP Ewald (src/gravity.cpp:733-785) */
-            const int32_t *lcp = LV.pool[TG_CP_E] + LV.off[TG_CP_E][i];
-            const int32_t ncp = LV.len[TG_CP_E][i];
-            const T m = T(P.m_d);
-            for (int32_t c = 0; c < ncp; c++) {
-                const int32_t src = lcp[c];
-                for (int32_t q = pb[src] + lane; q < pe[src]; q += 32) {
-                    const int4 y = pos[q];
-                    const int32_t yy[3] = {y.x, y.y, y.z};
-                    T dX[3], D[LP];
-#pragma unroll
-                    for (int d = 0; d < 3; d++) dX[d] = sep<T>(X[d], yy[d], true);
-                    green_ewald_full<T>(E, dX, D);
-                    contract_P2L<T, T>(L, m, D);
-                }
-            }
-        }
 #pragma unroll
         for (int k = 0; k < LP; k++) {
             const double v = warp_sum((double)L[k]);
@@ -352,6 +305,8 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
         }
     }
 }
+
+#include "tg_ewald_node.cuh"
 
 /* ---- L2L, one level ---- */
 __global__ void k_l2l(int64_t first, int64_t count, const int32_t *__restrict__ pb, const int32_t *__restrict__ pe,
@@ -658,6 +613,37 @@ static ListView listview(Solver &S) {
     return LV;
 }
 
+/* the node Ewald lists (CC_E, CP_E) of every node, in balanced chunks, added
+ * to Lloc */
+static int node_ewald(Solver &S, const GParams &P, const ListView &LV, const EwaldTables &E, bool f64,
+                      cudaStream_t st) {
+    const int64_t nn = S.nnodes;
+    TG_TRY(ensure(S.ew_cnt, (size_t)nn + 1));
+    TG_TRY(ensure(S.ew_off, (size_t)nn + 1));
+    k_node_ewald_count<<<(int)((nn + 1 + 127) / 128), 128, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, LV, S.ew_cnt.p);
+    TG_TRY(launched(S));
+    size_t stmp = 0;
+    TG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, stmp, S.ew_cnt.p, S.ew_off.p, (int)(nn + 1), st));
+    TG_TRY(ensure(S.cub_tmp, stmp));
+    TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, stmp, S.ew_cnt.p, S.ew_off.p, (int)(nn + 1), st));
+    int32_t total = 0;
+    TG_CUDA(cudaMemcpyAsync(&total, S.ew_off.p + nn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (total <= 0) return TG_OK;
+    TG_TRY(ensure(S.ew_part, (size_t)total * LP));
+    const int g = (int)(((int64_t)total * 32 + 127) / 128);
+    if (f64)
+        k_node_ewald<double><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                                E, S.ew_part.p);
+    else
+        k_node_ewald<float><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                               E, S.ew_part.p);
+    TG_TRY(launched(S));
+    k_node_ewald_reduce<<<(int)((nn * LP + 255) / 256), 256, 0, st>>>(nn, S.ew_off.p, S.ew_part.p, S.nd_Lloc.p);
+    TG_TRY(launched(S));
+    return TG_OK;
+}
+
 /* the leaf Ewald lists (PP_E, PC_E) of every leaf, in balanced chunks, added
  * to the FP64 accumulators accd (leaf_max <= 64) */
 static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const EwaldTables &E, bool f64,
@@ -713,6 +699,7 @@ int gravity_forces(Solver &S, cudaStream_t st) {
             k_node<float><<<g, TPB, 0, st>>>(P, nn, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV, E, S.nd_Lloc.p);
         TG_TRY(launched(S));
     }
+    if (S.prm.ewald) TG_TRY(node_ewald(S, P, LV, E, f64, st));
     for (int L = 0; L <= S.depth; L++) {
         const int64_t first = S.level_off[L], count = S.level_off[L + 1] - S.level_off[L];
         if (count <= 0) continue;
