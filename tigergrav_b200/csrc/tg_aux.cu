@@ -54,7 +54,8 @@ static std::vector<std::array<int, 3>> lattice(int n2max) {
 }
 
 /* periodic_parts (tigergrav/green.hpp:30-59) in FP64: one thread per h */
-__global__ void k_periodic_parts(const float4 *four, int nf, double scale, double *Hd, float *Hf) {
+__global__ void k_periodic_parts(const float4 *four, int nf, double scale, double *Hd, float *Hf, float4 *Pf,
+                                 double2 *Pd) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nf) return;
     const float4 hv = four[t];
@@ -92,9 +93,13 @@ __global__ void k_periodic_parts(const float4 *four, int nf, double scale, doubl
         }
     }
     for (int i = 0; i < LP; i++) {
-        Hd[LP * t + i] = scale * D[i];
-        Hf[LP * t + i] = (float)scale * F[i]; /* scale is a power of two: exact */
+        Hd[HS * t + i] = scale * D[i];
+        Hf[HS * t + i] = (float)scale * F[i]; /* scale is a power of two: exact */
     }
+    for (int i = LP; i < HS; i++) Hd[HS * t + i] = 0.0, Hf[HS * t + i] = 0.0f;
+    Pf[t] = make_float4(Hf[HS * t + E0()], Hf[HS * t + E1(0)], Hf[HS * t + E1(1)], Hf[HS * t + E1(2)]);
+    Pd[2 * t] = make_double2(Hd[HS * t + E0()], Hd[HS * t + E1(0)]);
+    Pd[2 * t + 1] = make_double2(Hd[HS * t + E1(1)], Hd[HS * t + E1(2)]);
 }
 
 int ewald_tables(Solver &S, cudaStream_t st) {
@@ -116,11 +121,14 @@ int ewald_tables(Solver &S, cudaStream_t st) {
     if ((int)f4.size() != NFOUR_HALF) return TG_ERR_STATE;
     TG_TRY(ensure(S.ew_real, NREAL));
     TG_TRY(ensure(S.ew_four, NFOUR_HALF));
-    TG_TRY(ensure(S.ew_Hf, NFOUR_HALF * LP));
-    TG_TRY(ensure(S.ew_Hd, NFOUR_HALF * LP));
+    TG_TRY(ensure(S.ew_Hf, NFOUR_HALF * HS));
+    TG_TRY(ensure(S.ew_Hd, NFOUR_HALF * HS));
+    TG_TRY(ensure(S.ew_Pf, NFOUR_HALF));
+    TG_TRY(ensure(S.ew_Pd, 2 * NFOUR_HALF));
     TG_CUDA(cudaMemcpyAsync(S.ew_real.p, r4.data(), sizeof(float4) * NREAL, cudaMemcpyHostToDevice, st));
     TG_CUDA(cudaMemcpyAsync(S.ew_four.p, f4.data(), sizeof(float4) * NFOUR_HALF, cudaMemcpyHostToDevice, st));
-    k_periodic_parts<<<(NFOUR_HALF + 63) / 64, 64, 0, st>>>(S.ew_four.p, NFOUR_HALF, 2.0, S.ew_Hd.p, S.ew_Hf.p);
+    k_periodic_parts<<<(NFOUR_HALF + 63) / 64, 64, 0, st>>>(S.ew_four.p, NFOUR_HALF, 2.0, S.ew_Hd.p, S.ew_Hf.p, S.ew_Pf.p,
+                                                            S.ew_Pd.p);
     TG_TRY(launched(S));
     TG_CUDA(cudaStreamSynchronize(st)); /* host vectors go out of scope */
     S.have_tables = true;

@@ -312,7 +312,7 @@ int tg_destroy(tg_solver *s) {
         release(S.nxt_pool[q]);
     }
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
-    release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd);
+    release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part);
     if (S.h_err) cudaFreeHost(S.h_err);
     if (S.h_cnt) cudaFreeHost(S.h_cnt);

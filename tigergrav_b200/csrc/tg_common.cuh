@@ -24,6 +24,7 @@ constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
 constexpr int NREAL_F32 = 123; /* |n|^2 <= 9: every n that can lie within the FP32 cut 2.2 of |X| <= sqrt(3)/2 */
 constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
 constexpr int NFOUR_HALF = 61; /* one of each pair +-h (h != 0) */
+constexpr int HS = 36;         /* row stride of the coefficient tables (16-byte rows) */
 constexpr float EWALD_RCUT = 1.0e-6f;
 constexpr float EWALD_PHI0 = 2.8372975f; /* r -> 0 limit (tigergrav/green.hpp:272) */
 
@@ -120,7 +121,7 @@ __device__ __forceinline__ double t_rcp(double x) { return 1.0 / x; }
  * approximation that the reference uses (tigergrav/simd.hpp:676-692), with
  * expf; FP64: the double-precision erfc and exp. */
 __device__ __forceinline__ float t_erfcexp(float x, float *e) {
-    const float t1 = __frcp_rn(1.0f + 0.3275911f * x);
+    const float t1 = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
     *e = __expf(-x * x);
     const float poly = t1 * (0.254829592f + t1 * (-0.284496736f + t1 * (1.421413741f + t1 * (-1.453152027f + t1 * 1.061405429f))));
     return poly * *e;
@@ -228,8 +229,10 @@ __device__ __forceinline__ void green_direct(const T *dX, T *D) {
 struct EwaldTables {
     const float4 *real; /* NREAL lattice vectors n by increasing |n|^2 (w = |n|^2) */
     const float4 *four; /* NFOUR_HALF reciprocal vectors h, first non-zero component > 0 (w unused) */
-    const float *Hf;    /* NFOUR_HALF x 35: 2 x periodic_parts coefficients, float */
-    const double *Hd;   /* NFOUR_HALF x 35, double */
+    const float *Hf;    /* NFOUR_HALF rows of HS: 2 x periodic_parts coefficients, float */
+    const double *Hd;   /* NFOUR_HALF rows of HS, double */
+    const float4 *Pf;   /* NFOUR_HALF x (H0, Hx, Hy, Hz): the potential and force terms, float */
+    const double2 *Pd;  /* NFOUR_HALF x 2, double */
 };
 
 /* Real-space cut of the Ewald sum.  The reference masks images at r >= 3.6
@@ -415,8 +418,26 @@ __device__ __forceinline__ void t_sincos2pi(double x, double *s, double *c) { si
  * the 61 vectors h with first non-zero component > 0: the terms of h and -h
  * are equal (H(h) is even/odd in h like cos/sin), so the table holds 2 H(h)
  * and each pair costs one term; h = 0 has H = 0. */
+/* one coefficient row (HS values) with 16-byte loads */
+__device__ __forceinline__ void load_row(const float *p, float *H) {
+#pragma unroll
+    for (int k = 0; k < HS / 4; k++) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(p) + k);
+        H[4 * k] = v.x, H[4 * k + 1] = v.y, H[4 * k + 2] = v.z, H[4 * k + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void load_row(const double *p, double *H) {
+#pragma unroll
+    for (int k = 0; k < HS / 2; k++) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + k);
+        H[2 * k] = v.x, H[2 * k + 1] = v.y;
+    }
+}
+
 template <class T>
-__device__ __forceinline__ void ewald_four_term(T *D, const T *X, float4 h, const T *H) {
+__device__ __forceinline__ void ewald_four_term(T *D, const T *X, float4 h, const T *Hrow) {
+    T H[HS];
+    load_row(Hrow, H);
     const T hdotdx = X[0] * T(h.x) + X[1] * T(h.y) + X[2] * T(h.z);
     T si, co;
     t_sincos2pi(hdotdx, &si, &co);

@@ -172,11 +172,18 @@ __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0
         const T hdotdx = dX0[0] * T(h.x) + dX0[1] * T(h.y) + dX0[2] * T(h.z);
         T s, c;
         t_sincos2pi(hdotdx, &s, &c);
-        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
-        ph += H[E0()] * c;
-        gx -= H[E1(0)] * s;
-        gy -= H[E1(1)] * s;
-        gz -= H[E1(2)] * s;
+        T H0, Hx, Hy, Hz;
+        if (sizeof(T) == 4) {
+            const float4 q = __ldg(&E.Pf[t]);
+            H0 = T(q.x), Hx = T(q.y), Hy = T(q.z), Hz = T(q.w);
+        } else {
+            const double2 q0 = __ldg(&E.Pd[2 * t]), q1 = __ldg(&E.Pd[2 * t + 1]);
+            H0 = T(q0.x), Hx = T(q0.y), Hy = T(q1.x), Hz = T(q1.y);
+        }
+        ph += H0 * c;
+        gx -= Hx * s;
+        gy -= Hy * s;
+        gz -= Hz * s;
     }
     const T rinv = t_rsqrt(r2);
     T p0, f0;
@@ -202,7 +209,7 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
     ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T>(D, mom, d, rr2); });
     ewald_mom_finish<T>(D, mom);
     for (int t = 0; t < NFOUR_HALF; t++) {
-        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
+        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
         ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
     ewald_finish<T, T>(D, X);
@@ -228,7 +235,7 @@ __device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *
     }
     ewald_mom_finish<T>(D, mom);
     for (int t = lane; t < NFOUR_HALF; t += 32) {
-        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + LP * t) : (const T *)(E.Hd + LP * t);
+        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
         ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
     if (lane == 0) ewald_finish<T, T>(D, X);
@@ -600,7 +607,7 @@ __global__ void k_seam_node(GParams P, int kind_ewald, int is_cc, int64_t ngroup
 }
 
 static EwaldTables tables(Solver &S) {
-    return EwaldTables{S.ew_real.p, S.ew_four.p, S.ew_Hf.p, S.ew_Hd.p};
+    return EwaldTables{S.ew_real.p, S.ew_four.p, S.ew_Hf.p, S.ew_Hd.p, S.ew_Pf.p, S.ew_Pd.p};
 }
 
 static ListView listview(Solver &S) {

@@ -115,6 +115,8 @@ struct Solver {
     DevBuf<float4> ew_real, ew_four;
     DevBuf<float> ew_Hf;
     DevBuf<double> ew_Hd;
+    DevBuf<float4> ew_Pf;
+    DevBuf<double2> ew_Pd;
     bool have_tables = false;
 
     /* events for phase timing */
