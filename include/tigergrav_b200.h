@@ -143,6 +143,25 @@ int tg_energy_noalloc(const float *v, const float *phi, int64_t n, double m, dou
 /* n_steps kick-drift-kick leapfrog steps of dt (first call computes forces if needed). */
 int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream);
 
+/* ---- differentiation (forward/backward pair, like torch.autograd.Function) ----
+ * No counterpart in the reference (its leapfrog, src/part_vect.cpp:341-540 driven
+ * by src/main.cpp:258-273, is forward only).
+ * tg_forward: n_steps leapfrog steps as tg_leapfrog, checkpointing positions and
+ * velocities (caller order) before the first step and after each step.
+ * tg_backward: given dL/dx and dL/dv after the last step (n x 3 doubles, caller
+ * order; gv may be NULL for zero) returns dL/dx and dL/dv before the first step
+ * (gv0 may be NULL).  Each step's Jacobian-vector product recomputes the tree,
+ * multipoles and lists at that step's checkpoint; see tg_tidal for the terms.
+ * Leaves the solver at the first checkpoint (tree and lists built, no forces).
+ * tg_tidal: out = J u with J = dg/dx (g the accelerations per unit G) at the
+ * current particles and lists (after tg_walk): far field through the local
+ * expansion's tidal tensor, PC through the multipoles' (monopole + quadrupole)
+ * tidal tensors, PP (direct and Ewald) through the exact pair Hessians acting
+ * on u_i - u_j. */
+int tg_forward(tg_solver *s, double dt, int n_steps, void *stream);
+int tg_backward(tg_solver *s, const double *gx, const double *gv, double *gx0, double *gv0, int where, void *stream);
+int tg_tidal(tg_solver *s, const double *u, double *out, int where, void *stream);
+
 int tg_get_stats(tg_solver *s, tg_stats *out);
 
 /* ---- introspection (parity tests) ----------------------------------- */

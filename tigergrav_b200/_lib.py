@@ -41,7 +41,7 @@ EXPORTS = [
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
-    "tg_energy_noalloc",
+    "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal",
 ]
 
 
@@ -93,6 +93,9 @@ def _load():
     L.tg_truth.argtypes = [vp, vp, i64, d, vp, vp, vp]
     L.tg_device_fp32_peak.argtypes = [i32, P(d), vp]
     L.tg_energy_noalloc.argtypes = [vp, vp, i64, d, d, vp, i32, vp]
+    L.tg_forward.argtypes = [vp, d, i32, vp]
+    L.tg_backward.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+    L.tg_tidal.argtypes = [vp, vp, vp, i32, vp]
     return L
 
 

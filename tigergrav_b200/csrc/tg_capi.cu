@@ -314,6 +314,8 @@ int tg_destroy(tg_solver *s) {
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
     release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part);
+    release(S.ck_x); release(S.ck_v); release(S.adj_x); release(S.adj_v); release(S.tid_u); release(S.tid_o);
+    release(S.tid_U); release(S.tid_V);
     if (S.h_err) cudaFreeHost(S.h_err);
     if (S.h_cnt) cudaFreeHost(S.h_cnt);
     if (S.h_stage) cudaFreeHost(S.h_stage);
@@ -477,6 +479,103 @@ int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream) {
         TG_TRY(tg_solve_gravity(s, stream));
         TG_TRY(tg_kick(s, 0.5 * dt, stream));
     }
+    return TG_OK;
+}
+
+/* ---- differentiation ---- */
+
+int tg_forward(tg_solver *s, double dt, int n_steps, void *stream) {
+    CHECK_HANDLE(s);
+    Solver &S = s->S;
+    if (n_steps < 0 || !std::isfinite(dt) || S.n <= 0) return TG_ERR_ARG;
+    cudaStream_t st = STREAM(stream);
+    const int64_t n = S.n;
+    TG_TRY(ensure(S.ck_x, (size_t)3 * n * (n_steps + 1)));
+    TG_TRY(ensure(S.ck_v, (size_t)3 * n * (n_steps + 1)));
+    S.ck_steps = -1;
+    if (!S.have_forces) TG_TRY(tg_solve_gravity(s, stream));
+    const int gn = (int)((n + 255) / 256);
+    k_unpack<<<gn, 256, 0, st>>>(n, S.pos.p, S.vel.p, S.ck_x.p, S.ck_v.p);
+    TG_TRY(launched(S));
+    for (int k = 0; k < n_steps; k++) {
+        TG_TRY(tg_kick(s, 0.5 * dt, stream));
+        TG_TRY(tg_drift(s, dt, stream));
+        TG_TRY(tg_solve_gravity(s, stream));
+        TG_TRY(tg_kick(s, 0.5 * dt, stream));
+        k_unpack<<<gn, 256, 0, st>>>(n, S.pos.p, S.vel.p, S.ck_x.p + (size_t)3 * n * (k + 1),
+                                     S.ck_v.p + (size_t)3 * n * (k + 1));
+        TG_TRY(launched(S));
+    }
+    S.ck_steps = n_steps;
+    S.ck_dt = dt;
+    return TG_OK;
+}
+
+/* tree, multipoles and lists at checkpoint k */
+static int at_checkpoint(tg_solver *s, int k, cudaStream_t st) {
+    Solver &S = s->S;
+    const int64_t n = S.n;
+    k_pack<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.ck_x.p + (size_t)3 * n * k, S.ck_v.p + (size_t)3 * n * k,
+                                                   S.pos.p, S.vel.p);
+    TG_TRY(launched(S));
+    S.have_tree = S.have_multipoles = S.have_lists = S.have_forces = false;
+    TG_TRY(tg_build(s, st));
+    TG_TRY(tg_multipoles(s, st));
+    TG_TRY(tg_walk(s, st));
+    return TG_OK;
+}
+
+int tg_backward(tg_solver *s, const double *gx, const double *gv, double *gx0, double *gv0, int where, void *stream) {
+    CHECK_HANDLE(s);
+    Solver &S = s->S;
+    if (S.ck_steps < 0) return TG_ERR_STATE;
+    if (!gx || !gx0 || (where != TG_HOST && where != TG_DEVICE)) return TG_ERR_ARG;
+    cudaStream_t st = STREAM(stream);
+    const int64_t n = S.n;
+    const size_t bytes = sizeof(double) * 3 * n;
+    const int K = S.ck_steps;
+    const double dt = S.ck_dt, G = S.prm.G;
+    TG_TRY(ensure(S.adj_x, 3 * n));
+    TG_TRY(ensure(S.adj_v, 3 * n));
+    const cudaMemcpyKind in = where == TG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind out = where == TG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    TG_CUDA(cudaMemcpyAsync(S.adj_x.p, gx, bytes, in, st));
+    if (gv) TG_CUDA(cudaMemcpyAsync(S.adj_v.p, gv, bytes, in, st));
+    else TG_CUDA(cudaMemsetAsync(S.adj_v.p, 0, bytes, st));
+    const int gn3 = (int)((3 * n + 255) / 256);
+    if (gv) {
+        TG_TRY(at_checkpoint(s, K, st));
+        TG_TRY(tidal_apply(S, S.adj_v.p, S.adj_x.p, 0.5 * dt * G, st));
+    }
+    for (int k = K - 1; k >= 0; k--) {
+        k_axpy3<<<gn3, 256, 0, st>>>(n, dt, S.adj_x.p, S.adj_v.p);
+        TG_TRY(launched(S));
+        TG_TRY(at_checkpoint(s, k, st));
+        TG_TRY(tidal_apply(S, S.adj_v.p, S.adj_x.p, (k > 0 ? dt : 0.5 * dt) * G, st));
+    }
+    TG_CUDA(cudaMemcpyAsync(gx0, S.adj_x.p, bytes, out, st));
+    if (gv0) TG_CUDA(cudaMemcpyAsync(gv0, S.adj_v.p, bytes, out, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
+int tg_tidal(tg_solver *s, const double *u, double *out, int where, void *stream) {
+    CHECK_HANDLE(s);
+    Solver &S = s->S;
+    if (!u || !out || (where != TG_HOST && where != TG_DEVICE)) return TG_ERR_ARG;
+    if (!S.have_lists) return TG_ERR_STATE;
+    cudaStream_t st = STREAM(stream);
+    const int64_t n = S.n;
+    const size_t bytes = sizeof(double) * 3 * n;
+    TG_TRY(ensure(S.adj_x, 3 * n));
+    TG_TRY(ensure(S.adj_v, 3 * n));
+    TG_CUDA(cudaMemcpyAsync(S.adj_v.p, u, bytes, where == TG_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                            st));
+    TG_CUDA(cudaMemsetAsync(S.adj_x.p, 0, bytes, st));
+    TG_TRY(tidal_apply(S, S.adj_v.p, S.adj_x.p, 1.0, st));
+    TG_CUDA(cudaMemcpyAsync(out, S.adj_x.p, bytes, where == TG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                            st));
+    TG_CUDA(cudaStreamSynchronize(st));
     return TG_OK;
 }
 

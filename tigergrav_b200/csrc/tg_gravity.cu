@@ -681,21 +681,12 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     return TG_OK;
 }
 
-int gravity_forces(Solver &S, cudaStream_t st) {
-    if (!S.have_lists) return TG_ERR_STATE;
-    TG_TRY(ewald_tables(S, st));
-    const int64_t nn = S.nnodes, n = S.n;
-    const GParams P = make_gparams(S.prm);
-    const EwaldTables E = tables(S);
-    const ListView LV = listview(S);
+/* the node stage: CC/CP (direct, then Ewald) into Lloc, then L2L top-down into nd_L */
+static int node_stage(Solver &S, const GParams &P, const ListView &LV, const EwaldTables &E, cudaStream_t st) {
+    const int64_t nn = S.nnodes;
     const bool f64 = S.prm.precision == TG_PREC_F64;
     TG_TRY(ensure(S.nd_Lloc, 35 * nn));
     TG_TRY(ensure(S.nd_L, 35 * nn));
-    const bool split_pp = !f64 && S.prm.leaf_max <= 64;
-    if (f64 || split_pp) TG_TRY(ensure(S.accd, 4 * n));
-    if (!f64) TG_TRY(ensure(S.acc, n));
-    S.pp_timed = false;
-    if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[3], st));
     {
         const int TPB = 128;
         const int64_t want = (nn * 32 + TPB - 1) / TPB;
@@ -714,6 +705,24 @@ int gravity_forces(Solver &S, cudaStream_t st) {
         k_l2l<<<g, 128, 0, st>>>(first, count, S.nd_pb.p, S.nd_pe.p, S.nd_parent.p, S.nd_ms.p, S.nd_Lloc.p, S.nd_L.p);
         TG_TRY(launched(S));
     }
+    return TG_OK;
+}
+
+int gravity_forces(Solver &S, cudaStream_t st) {
+    if (!S.have_lists) return TG_ERR_STATE;
+    TG_TRY(ewald_tables(S, st));
+    const int64_t nn = S.nnodes, n = S.n;
+    const GParams P = make_gparams(S.prm);
+    const EwaldTables E = tables(S);
+    const ListView LV = listview(S);
+    const bool f64 = S.prm.precision == TG_PREC_F64;
+    (void)nn;
+    const bool split_pp = !f64 && S.prm.leaf_max <= 64;
+    if (f64 || split_pp) TG_TRY(ensure(S.accd, 4 * n));
+    if (!f64) TG_TRY(ensure(S.acc, n));
+    S.pp_timed = false;
+    if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[3], st));
+    TG_TRY(node_stage(S, P, LV, E, st));
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[4], st));
     const int32_t nleaves = (int32_t)S.st.leaves;
     if (nleaves > 0) {

@@ -4,5 +4,6 @@
 #include "tg_tree.cu"
 #include "tg_walk.cu"
 #include "tg_gravity.cu"
+#include "tg_adjoint.cu"
 #include "tg_capi.cu"
 #include "tg_noalloc.cu"

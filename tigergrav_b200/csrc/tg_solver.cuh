@@ -110,6 +110,12 @@ struct Solver {
     size_t h_stage_bytes = 0;
 
     /* Ewald tables */
+    /* leapfrog checkpoints (caller order) and adjoint state */
+    DevBuf<int32_t> ck_x;
+    DevBuf<float> ck_v;
+    int ck_steps = -1;
+    double ck_dt = 0.0;
+    DevBuf<double> adj_x, adj_v, tid_u, tid_o, tid_U, tid_V;
     DevBuf<int32_t> ew_cnt, ew_off; /* leaf Ewald chunks per leaf, and their exclusive scan */
     DevBuf<double> ew_part;          /* 64 x 4 partial sums per chunk */
     DevBuf<float4> ew_real, ew_four;

@@ -158,6 +158,29 @@ class GravitySolver:
     def leapfrog(self, dt, n_steps, stream=None):
         check("tg_leapfrog", lib.tg_leapfrog(self.h, float(dt), int(n_steps), _stream(stream)))
 
+    # ---- differentiation ----
+    def forward(self, dt, n_steps, stream=None):
+        """n_steps leapfrog steps with checkpoints for backward()."""
+        check("tg_forward", lib.tg_forward(self.h, float(dt), int(n_steps), _stream(stream)))
+        return self
+
+    def backward(self, gx, gv=None, stream=None):
+        """(dL/dx0, dL/dv0) from dL/dx, dL/dv after the last forward() step (n x 3, caller order)."""
+        gx = np.ascontiguousarray(gx, np.float64)
+        gv = None if gv is None else np.ascontiguousarray(gv, np.float64)
+        gx0 = np.zeros((self.n, 3))
+        gv0 = np.zeros((self.n, 3))
+        check("tg_backward", lib.tg_backward(self.h, gx.ctypes.data, None if gv is None else gv.ctypes.data,
+                                             gx0.ctypes.data, gv0.ctypes.data, TG_HOST, _stream(stream)))
+        return gx0, gv0
+
+    def tidal(self, u, stream=None):
+        """J u (J = dg/dx per unit G) at the current particles and lists (n x 3, caller order)."""
+        u = np.ascontiguousarray(u, np.float64)
+        out = np.zeros((self.n, 3))
+        check("tg_tidal", lib.tg_tidal(self.h, u.ctypes.data, out.ctypes.data, TG_HOST, _stream(stream)))
+        return out
+
     def energy(self, stream=None) -> dict:
         out = np.zeros(5)
         check("tg_energy", lib.tg_energy(self.h, out.ctypes.data, _stream(stream)))
