@@ -162,6 +162,26 @@ int tg_forward(tg_solver *s, double dt, int n_steps, void *stream);
 int tg_backward(tg_solver *s, const double *gx, const double *gv, double *gx0, double *gv0, int where, void *stream);
 int tg_tidal(tg_solver *s, const double *u, double *out, int where, void *stream);
 
+/* ---- batches of independent boxes ---------------------------------------
+ * No counterpart in the reference (one box per run).  nboxes periodic unit
+ * boxes, box b with counts[b] particles, its own m = 1/counts[b] and
+ * soft_len = 0.02 counts[b]^(-1/3) (params->m and soft_len are ignored);
+ * theta, G, ewald, leaf_max, precision and device come from params.  Particle
+ * and force arrays are the boxes' arrays concatenated in box order.  Calls run
+ * the boxes concurrently on nstreams streams (one host thread each) and return
+ * when all are done.  tg_batch_autotune times one evaluation per box for each
+ * candidate leaf size (1..128) and keeps the fastest per box (chosen: nboxes
+ * ints, may be NULL). */
+typedef struct tg_batch tg_batch;
+int tg_batch_create(const tg_params *params, int32_t nboxes, const int64_t *counts, int32_t nstreams, tg_batch **out);
+int tg_batch_destroy(tg_batch *b);
+int64_t tg_batch_size(tg_batch *b);
+int tg_batch_set_particles(tg_batch *b, const int32_t *x, const float *v, int where);
+int tg_batch_autotune(tg_batch *b, const int32_t *leaf_sizes, int32_t nsizes, int32_t *chosen);
+int tg_batch_solve(tg_batch *b);
+int tg_batch_leapfrog(tg_batch *b, double dt, int n_steps);
+int tg_batch_get_forces(tg_batch *b, float *phi, float *g, int where);
+
 int tg_get_stats(tg_solver *s, tg_stats *out);
 
 /* ---- introspection (parity tests) ----------------------------------- */

@@ -5,11 +5,12 @@ this package is its host-side binding.  ``ics`` (seeded workloads) needs no GPU;
 ``GravitySolver`` and the kernel-level seams load the CUDA library on first use
 and raise if it is missing.
 """
-__all__ = ["GravitySolver", "make_params", "gravity_PP", "gravity_PC", "gravity_CC", "gravity_CP"]
+__all__ = ["GravitySolver", "GravityBatch", "make_params", "gravity_PP", "gravity_PC", "gravity_CC", "gravity_CP"]
 
 
 def __getattr__(name):
-    if name in ("GravitySolver", "make_params", "gravity_PP", "gravity_PC", "gravity_CC", "gravity_CP"):
+    if name in ("GravitySolver", "GravityBatch", "make_params", "gravity_PP", "gravity_PC", "gravity_CC",
+                "gravity_CP"):
         from . import solver
         return getattr(solver, name)
     raise AttributeError(name)

@@ -41,7 +41,9 @@ EXPORTS = [
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
-    "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal",
+    "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
+    "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
+    "tg_batch_get_forces",
 ]
 
 
@@ -96,6 +98,15 @@ def _load():
     L.tg_forward.argtypes = [vp, d, i32, vp]
     L.tg_backward.argtypes = [vp, vp, vp, vp, vp, i32, vp]
     L.tg_tidal.argtypes = [vp, vp, vp, i32, vp]
+    L.tg_batch_create.argtypes = [P(tg_params), i32, vp, i32, P(vp)]
+    L.tg_batch_destroy.argtypes = [vp]
+    L.tg_batch_size.restype = i64
+    L.tg_batch_size.argtypes = [vp]
+    L.tg_batch_set_particles.argtypes = [vp, vp, vp, i32]
+    L.tg_batch_autotune.argtypes = [vp, vp, i32, vp]
+    L.tg_batch_solve.argtypes = [vp]
+    L.tg_batch_leapfrog.argtypes = [vp, d, i32]
+    L.tg_batch_get_forces.argtypes = [vp, vp, vp, i32]
     return L
 
 

@@ -6,4 +6,5 @@
 #include "tg_gravity.cu"
 #include "tg_adjoint.cu"
 #include "tg_capi.cu"
+#include "tg_batch.cu"
 #include "tg_noalloc.cu"

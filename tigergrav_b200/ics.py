@@ -7,6 +7,7 @@ these workloads (its ``cosmos`` problem draws from ``rand()``,
 src/initialize.cpp:20-27), so these are this project's own:
 
 * ``uniform(n, seed)``     -- i.i.d. U[0,1)^3 from numpy's PCG64(seed).
+* ``batch(nboxes, seed)`` -- the uneven-box batch (see its docstring).
 * ``clustered(nside, seed)`` -- an nside^3 lattice displaced by the Zel'dovich
   displacement of a Gaussian random density field with P(k) ~ k^-2 (white
   noise from PCG64(seed), FFT on the nside^3 grid), scaled so that the rms
@@ -81,6 +82,23 @@ def batch_sizes(nboxes: int = 64, seed: int = 4, lo: float = 12.0, hi: float = 1
     """Box particle counts N = round(2^U[lo,hi])."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return np.round(2.0 ** rng.uniform(lo, hi, size=nboxes)).astype(np.int64)
+
+
+def batch(nboxes: int = 64, seed: int = 4):
+    """The batching workload: box counts from batch_sizes(nboxes, seed); even
+    boxes uniform (PCG64 seed 1000 + b), odd boxes clustered on the nearest
+    cube lattice (nside = round(N^(1/3)), seed 2000 + b).  Returns (counts,
+    positions of all boxes concatenated in box order)."""
+    sizes = batch_sizes(nboxes, seed)
+    counts, xs = [], []
+    for b, n in enumerate(sizes):
+        if b % 2 == 0:
+            x = uniform(int(n), 1000 + b)
+        else:
+            x = clustered(max(2, int(round(float(n) ** (1.0 / 3.0)))), 2000 + b)
+        counts.append(len(x))
+        xs.append(x)
+    return np.array(counts, np.int64), np.concatenate(xs)
 
 
 def default_soft_len(n: int) -> float:

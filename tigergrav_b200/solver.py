@@ -237,6 +237,65 @@ class GravitySolver:
         return phi, g
 
 
+class GravityBatch:
+    """Many independent periodic unit boxes (counts[b] particles each, m = 1/N_b,
+    soft_len = 0.02 N_b^-1/3) evaluated together on nstreams streams."""
+
+    def __init__(self, counts, theta=0.7, G=1.0, ewald=True, leaf_max=64, precision="f32", device=0, nstreams=8):
+        self.counts = np.ascontiguousarray(counts, np.int64)
+        self.n = int(self.counts.sum())
+        self.params = make_params(theta, 1.0, 1.0, G, ewald, leaf_max, precision, device)
+        h = C.c_void_p()
+        check("tg_batch_create", lib.tg_batch_create(C.byref(self.params), len(self.counts), self.counts.ctypes.data,
+                                                     int(nstreams), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib.tg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_particles(self, x, v=None):
+        x = np.ascontiguousarray(x, np.int32)
+        assert x.shape == (self.n, 3)
+        v = None if v is None else np.ascontiguousarray(v, np.float32)
+        check("tg_batch_set_particles", lib.tg_batch_set_particles(self.h, x.ctypes.data,
+                                                                   None if v is None else v.ctypes.data, TG_HOST))
+        return self
+
+    def autotune(self, leaf_sizes=(16, 32, 64, 128)):
+        ls = np.ascontiguousarray(leaf_sizes, np.int32)
+        chosen = np.zeros(len(self.counts), np.int32)
+        check("tg_batch_autotune", lib.tg_batch_autotune(self.h, ls.ctypes.data, len(ls), chosen.ctypes.data))
+        return chosen
+
+    def solve(self):
+        check("tg_batch_solve", lib.tg_batch_solve(self.h))
+        return self
+
+    def leapfrog(self, dt, n_steps):
+        check("tg_batch_leapfrog", lib.tg_batch_leapfrog(self.h, float(dt), int(n_steps)))
+        return self
+
+    def get_forces(self):
+        phi = np.zeros(self.n, np.float32)
+        g = np.zeros((self.n, 3), np.float32)
+        check("tg_batch_get_forces", lib.tg_batch_get_forces(self.h, phi.ctypes.data, g.ctypes.data, TG_HOST))
+        return phi, g
+
+
 def device_fp32_peak(device=0) -> float:
     """Measured FP32 FMA throughput of the device in TFLOP/s."""
     t = C.c_double(0)
