@@ -128,6 +128,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def reduce_over_ranks(v, op, device):
+    """max (slowest replica's time) or min of a value over the ranks of the
+    default process group (NCCL on the GPUs, gloo in the CPU tests)."""
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX if op == "max" else tdist.ReduceOp.MIN)
+    return float(t.item())
+
+
 def cpu_reference(x, theta, nthreads, budget_s=1.5, seed=1, walked=None):
     """Host time of one force evaluation with the reference's kernels (see the
     module docstring).  walked = (oracle, walk seconds) reuses a finished walk.
@@ -302,9 +312,7 @@ def main():
     step_ms, launches, clocks, stats = timed_steps(s, stream, flush, args.steps, args.warmup, args.dt, dev)
     total_ms = float(np.sum(step_ms))
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = reduce_over_ranks(total_ms, "max", "cuda")
         tdist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step * 1e-3) / 1e6
@@ -334,9 +342,7 @@ def main():
     e2e_step = float(np.mean(e2e_ms))
     e2e_val = world * n / (e2e_step * 1e-3) / 1e6
     if dist:
-        t = torch.tensor([e2e_val], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MIN)
-        e2e_val = float(t.item())
+        e2e_val = reduce_over_ranks(e2e_val, "min", "cuda")
 
     # ---- roofline of the dominant kernel ----
     peak = device_fp32_peak(dev)
