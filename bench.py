@@ -445,20 +445,31 @@ def bench_batch(args, w, cfg):
     return 0
 
 
+# DRAM bytes per interaction of each kernel, from the ncu capture summarised
+# in profiles/ewald_pp_kernels_clustered128_theta03.md (dram__bytes_read.sum +
+# dram__bytes_write.sum over its interactions); scaled by this run's counts,
+# assuming traffic in proportion to interactions (PC_E / CP_E at the rate of
+# PP_E / CC_E, which that capture does not contain).
+TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.2, "CP_E": 6.2}, "leaf": {"PP_E": 0.51, "PC_E": 0.51}}
+
+
 def roofline(phase_ms, cnt, peak):
     """FP32 roofline of the kernel with the largest share of the evaluation.
     achieved = executed FP32 operations (per-interaction counts from the
-    kernel source, FMA = 2) / that kernel's CUDA-event time."""
+    kernel source, FMA = 2) / that kernel's CUDA-event phase time."""
     leaf_far = max(phase_ms["leaves"] - phase_ms.get("pp", 0.0), 1e-9)
-    kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}),
-            "k_node<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS),
-            "k_leaf<float,64,false> (L2P, PC, PC/PP Ewald)": (leaf_far, LEAF_FLOPS)}
+    kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
+            "k_node + k_node_ewald<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
+            "k_ewald_chunk<float> + k_leaf<float,64,false> (PC/PP Ewald chunks, L2P, PC direct)":
+                (leaf_far, LEAF_FLOPS, "leaf")}
     name = max(kern, key=lambda k: kern[k][0])
-    ms, fl = kern[name]
+    ms, fl, tk = kern[name]
     flops = sum(cnt[k] * v for k, v in fl.items())
     achieved = flops / (ms * 1e-3) / 1e12
+    traffic = sum(cnt[k] * v for k, v in TRAFFIC[tk].items())
     return {"kernel": name, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": "ncu DRAM bytes per interaction at 128^3 theta 0.3, scaled by this run's counts",
             "peak_source": "measured FP32 FMA kernel on this GPU (tg_device_fp32_peak); MEASURED_PEAKS.json has no "
                            "FP32 figure",
             "flops_per_launch": flops, "flops_per_interaction": fl, "ms_per_launch": ms}
