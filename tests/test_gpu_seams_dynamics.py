@@ -1,0 +1,189 @@
+"""Kernel-level seams (tg_gravity_*, tigergrav/gravity.hpp:39-46), the 32^3
+plain-method configuration, and kick/drift (src/part_vect.cpp:341-540)
+against the CPU oracle."""
+import numpy as np
+import pytest
+
+from helpers import rel_force_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _groups(rng, ngroups, nsink, nsrc, spread=0.05):
+    """ngroups sink groups near random centres with sources around them."""
+    from tigergrav_b200 import ics
+    sx, yx = [], []
+    for _ in range(ngroups):
+        c = rng.random(3)
+        sx.append(ics.double_to_pos((c + spread * rng.standard_normal((nsink, 3))) % 1.0))
+        yx.append(ics.double_to_pos((c + 4 * spread * rng.standard_normal((nsrc, 3))) % 1.0))
+    return sx, yx
+
+
+def _k64(oracle_mod, name):
+    """the oracle's FP64 restatement of a kernel (tgo64_<name>)"""
+    import ctypes as C
+    fn = getattr(oracle_mod.lib(), "tgo64_" + name)
+    fn.restype = C.c_uint64
+    P, vp, i = C.POINTER(oracle_mod.Params), C.c_void_p, C.c_int
+    fn.argtypes = {"PP": [P, vp, vp, i, vp, i, i], "PC": [P, vp, vp, i, vp, vp, i], "CC": [P, vp, vp, vp, vp, i],
+                   "CP": [P, vp, vp, vp, i]}[name[:2]]
+    return fn
+
+
+def _pp64(oracle_mod, po, f, x, y):
+    import ctypes as C
+    x = np.ascontiguousarray(x, np.int32)
+    y = np.ascontiguousarray(y, np.int32)
+    _k64(oracle_mod, "PP_ewald")(C.byref(po), f.ctypes.data, x.ctypes.data, len(x), y.ctypes.data, len(y), 1)
+
+
+@pytest.mark.parametrize("kind", ["direct", "ewald"])
+def test_seam_pp_pc(kind, oracle_mod):
+    """PP and PC over three CSR sink groups: the GPU seam (FP32 path) against
+    the oracle's restated kernels, group by group."""
+    import torch
+    from tigergrav_b200 import solver as S
+    rng = np.random.default_rng(21)
+    n_per, ns = 40, 150
+    sx, yx = _groups(rng, 3, n_per, ns)
+    p = S.make_params(theta=0.7, soft_len=2e-3, m=1.0 / 4096, ewald=True)
+    po = oracle_mod.params(theta=0.7, soft_len=2e-3, m=1.0 / 4096, ewald=True)
+    dev = "cuda"
+    sink_x = torch.from_numpy(np.concatenate(sx)).to(dev)
+    src_x = torch.from_numpy(np.concatenate(yx)).to(dev)
+    sink_off = torch.tensor([0, n_per, 2 * n_per, 3 * n_per], dtype=torch.int64, device=dev)
+    src_off = torch.tensor([0, ns, 2 * ns, 3 * ns], dtype=torch.int64, device=dev)
+    f = torch.zeros((3 * n_per, 4), dtype=torch.float64, device=dev)
+    S.gravity_PP(kind, p, sink_off, sink_x, src_off, src_x, f)
+    fg = f.cpu().numpy()
+    for k in range(3):
+        fo = np.zeros((n_per, 4))
+        oracle_mod.pp(kind, po, fo, sx[k], yx[k], True)
+        e = rel_force_err(fg[k * n_per:(k + 1) * n_per, 1:], fo[:, 1:])
+        if kind == "direct":
+            assert np.percentile(e, 99) < 1e-5, np.percentile(e, 99)
+        else:
+            # the Ewald correction alone is a small smooth force: judge both FP32
+            # evaluations against the oracle's FP64 one
+            f64 = np.zeros((n_per, 4))
+            _pp64(oracle_mod, po, f64, sx[k], yx[k])
+            e_gpu = rel_force_err(fg[k * n_per:(k + 1) * n_per, 1:], f64[:, 1:])
+            e_o32 = rel_force_err(fo[:, 1:], f64[:, 1:])
+            assert np.percentile(e_gpu, 99) < max(1e-5, 1.5 * np.percentile(e_o32, 99)), (
+                np.percentile(e_gpu, 99), np.percentile(e_o32, 99))
+    # PC: sources as multipoles (random moments, monopole dominant)
+    ym = rng.standard_normal((3 * ns, 17)).astype(np.float32) * 1e-5
+    ym[:, 0] = np.abs(ym[:, 0]) * 100 + 1e-4
+    src_m = torch.from_numpy(ym).to(dev)
+    f.zero_()
+    S.gravity_PC(kind, p, sink_off, sink_x, src_off, src_m, src_x, f)
+    fg = f.cpu().numpy()
+    import ctypes as C
+    for k in range(3):
+        fo = np.zeros((n_per, 4))
+        oracle_mod.pc(kind, po, fo, sx[k], ym[k * ns:(k + 1) * ns], yx[k])
+        e = rel_force_err(fg[k * n_per:(k + 1) * n_per, 1:], fo[:, 1:])
+        if kind == "direct":
+            assert np.percentile(e, 99) < 1e-5, np.percentile(e, 99)
+            continue
+        # green_ewald in the reference's FP32 form loses its D2..D4 to cancellation
+        # at small separations (the n = 0 image against the direct 1/r); these
+        # random multipoles weight D3 and D4 strongly, so judge against FP64
+        f64 = np.zeros((n_per, 4))
+        xs, ms_, ys = (np.ascontiguousarray(sx[k], np.int32), np.ascontiguousarray(ym[k * ns:(k + 1) * ns]),
+                       np.ascontiguousarray(yx[k], np.int32))
+        _k64(oracle_mod, "PC_ewald")(C.byref(po), f64.ctypes.data, xs.ctypes.data, len(xs), ms_.ctypes.data,
+                                     ys.ctypes.data, len(ys))
+        e_gpu = rel_force_err(fg[k * n_per:(k + 1) * n_per, 1:], f64[:, 1:])
+        assert np.percentile(e_gpu, 99) < 1e-5, np.percentile(e_gpu, 99)
+
+
+@pytest.mark.parametrize("kind", ["direct", "ewald"])
+def test_seam_cc_cp(kind, oracle_mod):
+    import torch
+    from tigergrav_b200 import solver as S
+    rng = np.random.default_rng(22)
+    ng, ns = 4, 60
+    sx, yx = _groups(rng, ng, 1, ns, spread=0.08)
+    p = S.make_params(theta=0.7, soft_len=2e-3, m=1.0 / 4096, ewald=True)
+    po = oracle_mod.params(theta=0.7, soft_len=2e-3, m=1.0 / 4096, ewald=True)
+    dev = "cuda"
+    sink_x = torch.from_numpy(np.concatenate(sx)).to(dev)
+    src_x = torch.from_numpy(np.concatenate(yx)).to(dev)
+    src_off = torch.arange(0, ng * ns + 1, ns, dtype=torch.int64, device=dev)
+    ym = rng.standard_normal((ng * ns, 17)).astype(np.float32) * 1e-5
+    ym[:, 0] = np.abs(ym[:, 0]) * 100 + 1e-4
+    src_m = torch.from_numpy(ym).to(dev)
+    L = torch.zeros((ng, 35), dtype=torch.float64, device=dev)
+    S.gravity_CC(kind, p, sink_x, src_off, src_m, src_x, L)
+    Lc = L.cpu().numpy()
+    L.zero_()
+    S.gravity_CP(kind, p, sink_x, src_off, src_x, L)
+    Lp = L.cpu().numpy()
+    import ctypes as C
+    for k in range(ng):
+        xs = np.ascontiguousarray(sx[k][0], np.int32)
+        ys = np.ascontiguousarray(yx[k], np.int32)
+        ms_ = np.ascontiguousarray(ym[k * ns:(k + 1) * ns])
+        lo = np.zeros(35)
+        if kind == "direct":
+            oracle_mod.cc(kind, po, lo, xs, ms_, ys)
+        else:  # FP64 reference, as for PC above
+            _k64(oracle_mod, "CC_ewald")(C.byref(po), lo.ctypes.data, xs.ctypes.data, ms_.ctypes.data,
+                                         ys.ctypes.data, len(ys))
+        assert np.abs(Lc[k] - lo).max() <= 2e-5 * np.abs(lo).max(), np.abs(Lc[k] - lo).max() / np.abs(lo).max()
+        lo = np.zeros(35)
+        if kind == "direct":
+            oracle_mod.cp(kind, po, lo, xs, ys)
+        else:
+            _k64(oracle_mod, "CP_ewald")(C.byref(po), lo.ctypes.data, xs.ctypes.data, ys.ctypes.data, len(ys))
+        assert np.abs(Lp[k] - lo).max() <= 2e-5 * np.abs(lo).max(), np.abs(Lp[k] - lo).max() / np.abs(lo).max()
+
+
+def test_config0_uniform32k(oracle_mod, has_ref):
+    """32^3 = 32768 uniform particles (seed 1), theta 0.7, Ewald on: per-particle
+    force and potential of the FP32 path against the reference's own kernels
+    (or the restated ones when the reference could not be built)."""
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.uniform(32768, 1)
+    with tg.GravitySolver(len(x), theta=0.7) as s:
+        s.set_particles(x).solve_gravity()
+        phi, g = s.get_forces()
+    o = oracle_mod.Oracle(theta=0.7).set_particles(x)
+    o.build().multipoles().walk().evaluate(use_ref=has_ref)
+    ophi, og = o.forces()
+    e = rel_force_err(g, og)
+    assert np.percentile(e, 99) < 1e-5, np.percentile(e, 99)
+    assert np.abs(phi - ophi).max() / np.sqrt(np.mean(ophi ** 2)) < 5e-5
+
+
+def test_leapfrog_matches_oracle(oracle_mod):
+    """Three KDK steps of the FP64 path against the oracle's FP64 forces with
+    its kick/drift restatement: positions within a few fixed-point units,
+    velocities and energies to 1e-7 relative."""
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.clustered(16, 3)
+    n = len(x)
+    dt, steps = 1e-3, 3
+    with tg.GravitySolver(n, theta=0.7, precision="f64") as s:
+        s.set_particles(x)
+        s.leapfrog(dt, steps)
+        xg, vg = s.get_particles()
+        eg = s.energy()
+    o = oracle_mod.Oracle(theta=0.7).set_particles(x)
+    o.build().multipoles().walk().evaluate(fp64=True)
+    for _ in range(steps):
+        o.kick(0.5 * dt)
+        o.drift(dt)
+        o.build().multipoles().walk().evaluate(fp64=True)
+        o.kick(0.5 * dt)
+    xo, vo = o.particles()
+    eo = o.energy()
+    dxi = (xg.astype(np.int64) - xo.astype(np.int64) + 2 ** 31) % 2 ** 32 - 2 ** 31
+    assert np.abs(dxi).max() <= 64, np.abs(dxi).max()
+    assert np.abs(vg - vo).max() <= 1e-6 * np.abs(vo).max()
+    assert abs(eg["ekin"] - eo[0]) <= 1e-6 * abs(eo[0])
+    assert abs(eg["epot"] - eo[1]) <= 1e-6 * abs(eo[1])

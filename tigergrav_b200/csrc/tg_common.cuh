@@ -269,26 +269,9 @@ template <class T> struct EwaldMom {
     }
 };
 
-/* One real-space image (tigergrav/green.hpp:212-236), alpha = 2, at
- * separation dx with |dx|^2 = r2 inside the cut. */
+/* add one image's radial factors d0..d4 at separation dx to the sums */
 template <class T>
-__device__ __forceinline__ void ewald_real_image(T *D, EwaldMom<T> &m, const T *dx, T r2) {
-    const T rinv = t_rsqrt(r2);
-    const T r = r2 * rinv;
-    const T r2inv = rinv * rinv;
-    const T r3inv = r2inv * rinv;
-    const T r5inv = r2inv * r3inv;
-    const T r7inv = r2inv * r5inv;
-    const T r9inv = r2inv * r7inv;
-    const T r4 = r2 * r2;
-    T expfac;
-    const T erfc = t_erfcexp(T(2) * r, &expfac);
-    const T expfactor = T(2.2567583341910252) * r * expfac; /* 4/sqrt(pi) */
-    const T d0 = -erfc * rinv;
-    const T d1 = (expfactor + erfc) * r3inv;
-    const T d2 = -fma(expfactor, fma(T(8), r2, T(3)), T(3) * erfc) * r5inv;
-    const T d3 = fma(expfactor, (T(15) + fma(T(40), r2, T(64) * r4)), T(15) * erfc) * r7inv;
-    const T d4 = -fma(expfactor, fma(T(8) * r2, (T(35) + fma(T(56), r2, T(64) * r4)), T(105)), T(105) * erfc) * r9inv;
+__device__ __forceinline__ void ewald_radial_add(T *D, EwaldMom<T> &m, const T *dx, T d0, T d1, T d2, T d3, T d4) {
     D[E0()] += d0;
     m.u1 += d1;
     m.s2 += d2;
@@ -311,6 +294,92 @@ __device__ __forceinline__ void ewald_real_image(T *D, EwaldMom<T> &m, const T *
             }
         }
     }
+}
+
+/* radial factors of one real-space image, -erfc(2r)/r and (1/r d/dr)^k of it
+ * (tigergrav/green.hpp:212-236), alpha = 2 */
+template <class T>
+__device__ __forceinline__ void ewald_image_factors(T r2, T &d0, T &d1, T &d2, T &d3, T &d4) {
+    const T rinv = t_rsqrt(r2);
+    const T r = r2 * rinv;
+    const T r2inv = rinv * rinv;
+    const T r3inv = r2inv * rinv;
+    const T r5inv = r2inv * r3inv;
+    const T r7inv = r2inv * r5inv;
+    const T r9inv = r2inv * r7inv;
+    const T r4 = r2 * r2;
+    T expfac;
+    const T erfc = t_erfcexp(T(2) * r, &expfac);
+    const T expfactor = T(2.2567583341910252) * r * expfac; /* 4/sqrt(pi) */
+    d0 = -erfc * rinv;
+    d1 = (expfactor + erfc) * r3inv;
+    d2 = -fma(expfactor, fma(T(8), r2, T(3)), T(3) * erfc) * r5inv;
+    d3 = fma(expfactor, (T(15) + fma(T(40), r2, T(64) * r4)), T(15) * erfc) * r7inv;
+    d4 = -fma(expfactor, fma(T(8) * r2, (T(35) + fma(T(56), r2, T(64) * r4)), T(105)), T(105) * erfc) * r9inv;
+}
+
+/* One real-space image (tigergrav/green.hpp:212-236) at separation dx with
+ * |dx|^2 = r2 inside the cut. */
+template <class T>
+__device__ __forceinline__ void ewald_real_image(T *D, EwaldMom<T> &m, const T *dx, T r2) {
+    T d0, d1, d2, d3, d4;
+    ewald_image_factors<T>(r2, d0, d1, d2, d3, d4);
+    ewald_radial_add<T>(D, m, dx, d0, d1, d2, d3, d4);
+}
+
+/* Taylor coefficients of (1/r d/dr)^k [erf(2r)/r] in u = r^2 (k = 0..4):
+ * erf(2r)/r = (4/sqrt(pi)) sum_n (-4u)^n / (n! (2n+1)), and (1/r d/dr) = 2 d/du,
+ * so row k holds 2^k a_{m+k} (m+k)!/m! for m = 0..13 (from the series of erf). */
+constexpr int EO_TERMS = 14;
+__constant__ float c_eo_f[5][EO_TERMS] = {
+    {2.256758334e+00f, -3.009011112e+00f, 3.610813335e+00f, -3.438869843e+00f, 2.674676544e+00f, -1.750697374e+00f,
+     9.875728779e-01f, -4.890837109e-01f, 2.157722254e-01f, -8.580415981e-02f, 3.105293403e-02f, -1.031006505e-02f,
+     3.161753283e-03f, -9.007844111e-04f},
+    {-6.018022225e+00f, 1.444325334e+01f, -2.063321906e+01f, 2.139741235e+01f, -1.750697374e+01f, 1.185087453e+01f,
+     -6.847171953e+00f, 3.452355607e+00f, -1.544474877e+00f, 6.210586806e-01f, -2.268214312e-01f, 7.588207879e-02f,
+     -2.342039469e-02f, 6.709290786e-03f},
+    {2.888650668e+01f, -8.253287622e+01f, 1.283844741e+02f, -1.400557900e+02f, 1.185087453e+02f, -8.216606344e+01f,
+     4.833297849e+01f, -2.471159803e+01f, 1.117905625e+01f, -4.536428623e+00f, 1.669405733e+00f, -5.620894725e-01f,
+     1.744415604e-01f, -5.021146653e-02f},
+    {-1.650657524e+02f, 5.135378965e+02f, -8.403347397e+02f, 9.480699628e+02f, -8.216606344e+02f, 5.799957419e+02f,
+     -3.459623724e+02f, 1.788649000e+02f, -8.165571522e+01f, 3.338811467e+01f, -1.236596840e+01f, 4.186597450e+00f,
+     -1.305498130e+00f, 3.773467787e-01f},
+    {1.027075793e+03f, -3.361338959e+03f, 5.688419777e+03f, -6.573285075e+03f, 5.799957419e+03f, -4.151548468e+03f,
+     2.504108600e+03f, -1.306491443e+03f, 6.009860640e+02f, -2.473193679e+02f, 9.210514391e+01f, -3.133195511e+01f,
+     9.811016247e+00f, -2.846272845e+00f},
+};
+
+/* FP32: the n = 0 image together with the removal of the direct 1/r that
+ * green_ewald's final assembly performs (tigergrav/green.hpp:265-285):
+ * radial factors of erf(2r)/r.  In the reference's form the two parts cancel
+ * to a factor r^(2k+1) in the k-th derivative (9 decimal digits of D4 at
+ * r = 0.1, more than FP32 holds); below r = 0.6 the Taylor series above is
+ * used instead, above it the difference of the closed forms loses < 35x. */
+__device__ __forceinline__ void ewald_origin_add(float *D, EwaldMom<float> &m, const float *dx, float r2) {
+    float c[5];
+    if (r2 < 0.36f) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            float v = c_eo_f[k][EO_TERMS - 1];
+#pragma unroll
+            for (int q = EO_TERMS - 2; q >= 0; q--) v = fmaf(v, r2, c_eo_f[k][q]);
+            c[k] = v;
+        }
+    } else {
+        ewald_image_factors<float>(r2, c[0], c[1], c[2], c[3], c[4]);
+        const float rinv = rsqrtf(r2), r2inv = rinv * rinv;
+        float dd = -rinv; /* direct: -1/r and its (1/r d/dr)^k: 1/r^3, -3/r^5, 15/r^7, -105/r^9 */
+        c[0] -= dd;
+        dd = rinv * r2inv;
+        c[1] -= dd;
+        dd *= -3.0f * r2inv;
+        c[2] -= dd;
+        dd *= -5.0f * r2inv;
+        c[3] -= dd;
+        dd *= -7.0f * r2inv;
+        c[4] -= dd;
+    }
+    ewald_radial_add<float>(D, m, dx, c[0], c[1], c[2], c[3], c[4]);
 }
 
 /* fold the delta terms of the image sums into D (once per evaluation) */

@@ -206,13 +206,22 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
     }
     EwaldMom<T> mom;
     mom.init();
-    ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T>(D, mom, d, rr2); });
+    if constexpr (sizeof(T) == 4) {
+        /* FP32: the n = 0 image carries the removal of the direct 1/r */
+        ewald_images<T>(X, [&](const T *d, T rr2, bool origin) {
+            if (origin) ewald_origin_add(D, mom, d, rr2);
+            else ewald_real_image<T>(D, mom, d, rr2);
+        });
+    } else {
+        ewald_images<T>(X, [&](const T *d, T rr2, bool) { ewald_real_image<T>(D, mom, d, rr2); });
+    }
     ewald_mom_finish<T>(D, mom);
     for (int t = 0; t < NFOUR_HALF; t++) {
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
         ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
-    ewald_finish<T, T>(D, X);
+    if constexpr (sizeof(T) == 4) D[E0()] += T(0.78539816339744831); /* pi/4 (tigergrav/green.hpp:270) */
+    else ewald_finish<T, T>(D, X);
 }
 
 /* green_ewald(dX) split over a warp: this lane's share of the real-space
@@ -231,14 +240,24 @@ __device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *
         const float4 n = __ldg(&E.real[t]);
         const T dx[3] = {X[0] - T(n.x), X[1] - T(n.y), X[2] - T(n.z)};
         const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
-        if (r2 < ewald_rcut2<T>() && n.w <= 17.0f) ewald_real_image<T>(D, mom, dx, r2);
+        if (r2 < ewald_rcut2<T>() && n.w <= 17.0f) {
+            if constexpr (sizeof(T) == 4) {
+                if (n.w == 0.0f) ewald_origin_add(D, mom, dx, r2);
+                else ewald_real_image<T>(D, mom, dx, r2);
+            } else {
+                ewald_real_image<T>(D, mom, dx, r2);
+            }
+        }
     }
     ewald_mom_finish<T>(D, mom);
     for (int t = lane; t < NFOUR_HALF; t += 32) {
         const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
         ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
     }
-    if (lane == 0) ewald_finish<T, T>(D, X);
+    if (lane == 0) {
+        if constexpr (sizeof(T) == 4) D[E0()] += T(0.78539816339744831);
+        else ewald_finish<T, T>(D, X);
+    }
 }
 
 /* CC/CP Ewald lists shorter than this are evaluated one source at a time by
