@@ -245,6 +245,10 @@ struct EwaldTables {
 template <class T> __device__ __forceinline__ T ewald_rcut2();
 template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 4.84f; }
 template <> __device__ __forceinline__ double ewald_rcut2<double>() { return 12.96; }
+/* PP Ewald needs only the potential and force factors d0, d1: an image at
+ * r >= 2 adds at most 8e-9 to d0 and 7e-8 to d1, so the FP32 path stops at 2
+ * there (~34 images) */
+template <class T> __device__ __forceinline__ T ewald_rcut2_pp() { return sizeof(T) == 4 ? T(4.0) : ewald_rcut2<T>(); }
 
 /* Sums over the real-space images that green_ewald's derivative tensors are
  * built from (tigergrav/green.hpp:62-117 applied per image, 212-236): with
@@ -422,8 +426,7 @@ __device__ __forceinline__ void ewald_mom_finish(T *D, const EwaldMom<T> &m) {
  * diverging at every level of the nest.  fn(dx, r2, is_origin) is called
  * once per image.  Caller guarantees |X| > 1e-6 (the reference's zmask = 1). */
 template <class T, class F>
-__device__ __forceinline__ void ewald_images(const T *X, F &&fn) {
-    const T R2 = ewald_rcut2<T>();
+__device__ __forceinline__ void ewald_images(const T *X, F &&fn, T R2 = ewald_rcut2<T>()) {
     const T R = t_sqrt(R2);
     int nx = (int)ceil(X[0] - R) - 1;
     const int nx1 = (int)floor(X[0] + R);

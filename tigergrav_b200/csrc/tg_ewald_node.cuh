@@ -18,7 +18,7 @@
 constexpr int EN_KCC = 128; /* CC_E source nodes per chunk (4 per lane) */
 constexpr int EN_KCP = 4;   /* CP_E source leaves per chunk */
 #ifndef EN_MINB
-#define EN_MINB 4 /* resident 128-thread blocks per SM the kernel is compiled for */
+#define EN_MINB 6 /* resident 128-thread blocks per SM the kernel is compiled for */
 #endif
 
 __global__ void k_node_ewald_count(int64_t nn, const int32_t *__restrict__ pb, const int32_t *__restrict__ pe,
@@ -51,7 +51,10 @@ __global__ void __launch_bounds__(128, EN_MINB) k_node_ewald(GParams P, int64_t 
     const int64_t i = lo;
     const int32_t k = c - off[i];
     const int32_t X[3] = {ms[i].x[0], ms[i].x[1], ms[i].x[2]};
-    T L[LP];
+    /* each lane's expansion sums live in shared memory (odd stride LP: no bank
+     * conflicts), which leaves the registers to the green_ewald evaluation */
+    __shared__ T sL[128 * LP];
+    T *L = sL + threadIdx.x * LP;
 #pragma unroll
     for (int q = 0; q < LP; q++) L[q] = T(0);
     const int32_t ncc = LV.len[TG_CC_E][i];

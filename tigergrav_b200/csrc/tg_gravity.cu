@@ -166,7 +166,7 @@ __device__ __forceinline__ void pp_ewald_pair(const EwaldTables &E, const T *dX0
         gx -= dx * d1;
         gy -= dy * d1;
         gz -= dz * d1;
-    });
+    }, ewald_rcut2_pp<T>());
     for (int t = 0; t < NFOUR_HALF; t++) {
         const float4 h = __ldg(&E.four[t]);
         const T hdotdx = dX0[0] * T(h.x) + dX0[1] * T(h.y) + dX0[2] * T(h.z);
