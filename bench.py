@@ -66,13 +66,13 @@ PP_FLOPS = 26
 # FP32 operations per interaction of the Ewald and multipole kernels, counted
 # from the source the same way.  One real-space image: separation and r^2 8,
 # rsqrt and powers of 1/r 8, erfc/exp 18, d0..d4 31, the moment sums 120 ->
-# 185; 44.6 images on average inside the FP32 cut r < 2.2 (4/3 pi 2.2^3).
+# 185; 38.8 images on average inside the FP32 cut r < 2.1 (4/3 pi 2.1^3).
 # One reciprocal term of the half sum: h.X 5, reduction and sin/cos 5, 35
-# FMAs 70 -> 80; 61 terms.  Finish 105.  green_ewald = 13.2k.  Contractions:
+# FMAs 70 -> 80; 61 terms.  Finish 105.  green_ewald = 12.2k.  Contractions:
 # M2L 858, M2P 414, P2L 70 (direct kernels: the reference's constants).
 # PP_E pair (cut r < 2, origin separate): 32.5 images x 44 + 61 x 18 + 30 = 2.6k.
-NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 14100, "CP_E": 13300}
-LEAF_FLOPS = {"PC_D": 581, "PC_E": 13600, "PP_E": 2600}
+NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 13100, "CP_E": 12300}
+LEAF_FLOPS = {"PC_D": 581, "PC_E": 12600, "PP_E": 2600}
 
 
 def make_particles(w):

@@ -21,7 +21,7 @@ constexpr int LP = 35;
 constexpr double POS_MAX = 4294967296.0;
 constexpr double POS_INV = 1.0 / 4294967296.0;
 constexpr int NREAL = 305;  /* |n|^2 <= 17 (tigergrav/green.hpp:3,8-28) */
-constexpr int NREAL_F32 = 123; /* |n|^2 <= 9: every n that can lie within the FP32 cut 2.2 of |X| <= sqrt(3)/2 */
+constexpr int NREAL_F32 = 123; /* |n|^2 <= 9: every n that can lie within the FP32 cut 2.1 of |X| <= sqrt(3)/2 */
 constexpr int NFOUR = 123;  /* |h|^2 <= 9 */
 constexpr int NFOUR_HALF = 61; /* one of each pair +-h (h != 0) */
 constexpr int HS = 36;         /* row stride of the coefficient tables (16-byte rows) */
@@ -236,17 +236,18 @@ struct EwaldTables {
 };
 
 /* Real-space cut of the Ewald sum.  The reference masks images at r >= 3.6
- * (tigergrav/green.hpp:220); the FP64 path keeps that.  An image at r >= 2.2
- * adds at most 1.1e-6 to the fourth derivative and 1e-8 to the potential
- * and force factors (erfc(4.4) = 3e-10; exp(-19.4) times the derivative
- * polynomials), i.e. below 1e-7 of each derivative of green_ewald and below
- * the error of the reference's own A&S erfc (1.5e-7); the FP32 path stops
- * there and evaluates ~45 images instead of ~200. */
+ * (tigergrav/green.hpp:220); the FP64 path keeps that.  The FP32 path stops
+ * at r = 2.1 (~39 images instead of ~200): an image there adds 3e-9 to D0 and
+ * 1.1e-8 to the force factor d1 (erfc(4.2) = 3e-9, exp(-17.6) times the
+ * derivative polynomials) -- below the error of the reference's own erfc
+ * (A&S 7.1.26, 1.5e-7 absolute) -- and its higher derivatives (d4 <= 1e-5)
+ * enter forces only through multipole moments and expansion offsets of leaf
+ * size. */
 template <class T> __device__ __forceinline__ T ewald_rcut2();
-template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 4.84f; }
+template <> __device__ __forceinline__ float ewald_rcut2<float>() { return 4.41f; }
 template <> __device__ __forceinline__ double ewald_rcut2<double>() { return 12.96; }
 /* PP Ewald needs only the potential and force factors d0, d1: an image at
- * r >= 2 adds at most 8e-9 to d0 and 7e-8 to d1, so the FP32 path stops at 2
+ * r >= 2 adds at most 8e-9 to d0 and 6e-8 to d1, so the FP32 path stops at 2
  * there (~34 images) */
 template <class T> __device__ __forceinline__ T ewald_rcut2_pp() { return sizeof(T) == 4 ? T(4.0) : ewald_rcut2<T>(); }
 
@@ -422,7 +423,7 @@ __device__ __forceinline__ void ewald_mom_finish(T *D, const EwaldMom<T> &m) {
  * integer ranges that the cut allows instead of testing all 305 vectors.
  * The three nested ranges are flattened into one loop that advances each
  * lane to its next image, so a warp whose lanes hold different X runs the
- * image body together (about 45 images per lane in FP32, in lockstep) instead of
+ * image body together (about 39 images per lane in FP32, in lockstep) instead of
  * diverging at every level of the nest.  fn(dx, r2, is_origin) is called
  * once per image.  Caller guarantees |X| > 1e-6 (the reference's zmask = 1). */
 template <class T, class F>
