@@ -162,6 +162,22 @@ int tg_forward(tg_solver *s, double dt, int n_steps, void *stream);
 int tg_backward(tg_solver *s, const double *gx, const double *gv, double *gx0, double *gv0, int where, void *stream);
 int tg_tidal(tg_solver *s, const double *u, double *out, int where, void *stream);
 
+/* ---- cosmological kick and drift factors ----------------------------------
+ * cosmos::advance_to_time / cosmo_advance (src/cosmo.cpp:50-106,187-218): the
+ * Friedmann expansion a(t) with a'' = H0^2 (-omega_m / (2 a^2) + omega_lambda a),
+ * integrated by the reference's fixed-step RK4.  state = {a, da/dt, tau}; one
+ * call advances it by dt and returns factors = {int_t^{t+dt/2} dt'/a,
+ * int_t^{t+dt} dt'/a^2, int_{t+dt/2}^{t+dt} dt'/a}: the first half kick, the
+ * drift and the second half kick, to be passed as dt to tg_kick / tg_drift.
+ * Host only (no GPU needed).  tg_leapfrog_cosmo runs n_steps such steps. */
+typedef struct tg_cosmo_params {
+    double H0;            /* Hubble constant in code units */
+    double omega_m;
+    double omega_lambda;
+} tg_cosmo_params;
+int tg_cosmo_kdk(const tg_cosmo_params *p, double *state, double dt, double *factors);
+int tg_leapfrog_cosmo(tg_solver *s, const tg_cosmo_params *p, double *state, double dt, int n_steps, void *stream);
+
 /* ---- batches of independent boxes ---------------------------------------
  * No counterpart in the reference (one box per run).  nboxes periodic unit
  * boxes, box b with counts[b] particles, its own m = 1/counts[b] and

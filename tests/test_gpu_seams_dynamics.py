@@ -187,3 +187,21 @@ def test_leapfrog_matches_oracle(oracle_mod):
     assert np.abs(vg - vo).max() <= 1e-6 * np.abs(vo).max()
     assert abs(eg["ekin"] - eo[0]) <= 1e-6 * abs(eo[0])
     assert abs(eg["epot"] - eo[1]) <= 1e-6 * abs(eo[1])
+
+
+def test_cosmo_leapfrog_static_limit():
+    """with a constant scale factor the comoving KDK factors are dt/2, dt, dt/2:
+    tg_leapfrog_cosmo then equals tg_leapfrog"""
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.clustered(16, 3)
+    n = len(x)
+    with tg.GravitySolver(n, theta=0.7, precision="f64") as s1, tg.GravitySolver(n, theta=0.7, precision="f64") as s2:
+        s1.set_particles(x).leapfrog(1e-3, 3)
+        s2.set_particles(x)
+        st = s2.leapfrog_cosmo(1e-3, 3, [1.0, 1e-12, 0.0], H0=1e-6, omega_m=0.0, omega_lambda=0.0)
+        x1, v1 = s1.get_particles()
+        x2, v2 = s2.get_particles()
+    assert abs(st[0] - 1.0) < 1e-9
+    assert np.abs(x1.astype(np.int64) - x2.astype(np.int64)).max() <= 2
+    assert np.abs(v1 - v2).max() <= 1e-6 * np.abs(v1).max()

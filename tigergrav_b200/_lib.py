@@ -25,6 +25,10 @@ class tg_params(C.Structure):
                 ("ewald", C.c_int32), ("leaf_max", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32)]
 
 
+class tg_cosmo_params(C.Structure):
+    _fields_ = [("H0", C.c_double), ("omega_m", C.c_double), ("omega_lambda", C.c_double)]
+
+
 class tg_stats(C.Structure):
     _fields_ = [("n", C.c_int64), ("nodes", C.c_int64), ("leaves", C.c_int64), ("depth", C.c_int32),
                 ("walk_retries", C.c_int32), ("ref_stats", C.c_uint64 * 6), ("counts", C.c_uint64 * 8),
@@ -43,7 +47,7 @@ EXPORTS = [
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
-    "tg_batch_get_forces",
+    "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo",
 ]
 
 
@@ -107,6 +111,8 @@ def _load():
     L.tg_batch_solve.argtypes = [vp]
     L.tg_batch_leapfrog.argtypes = [vp, d, i32]
     L.tg_batch_get_forces.argtypes = [vp, vp, vp, i32]
+    L.tg_cosmo_kdk.argtypes = [P(tg_cosmo_params), vp, d, vp]
+    L.tg_leapfrog_cosmo.argtypes = [vp, P(tg_cosmo_params), vp, d, i32, vp]
     return L
 
 

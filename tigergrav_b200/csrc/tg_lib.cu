@@ -7,4 +7,5 @@
 #include "tg_adjoint.cu"
 #include "tg_capi.cu"
 #include "tg_batch.cu"
+#include "tg_cosmo.cu"
 #include "tg_noalloc.cu"

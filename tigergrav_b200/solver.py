@@ -27,7 +27,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import lib, check, tg_params, tg_stats, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, LIST_KINDS
+from ._lib import lib, check, tg_params, tg_stats, tg_cosmo_params, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, \
+    LIST_KINDS
 
 
 def _is_torch_cuda(a) -> bool:
@@ -181,6 +182,14 @@ class GravitySolver:
         check("tg_tidal", lib.tg_tidal(self.h, u.ctypes.data, out.ctypes.data, TG_HOST, _stream(stream)))
         return out
 
+    def leapfrog_cosmo(self, dt, n_steps, state, H0, omega_m=0.3, omega_lambda=0.7, stream=None):
+        """n_steps comoving KDK steps with the cosmological factors; state = [a, da/dt, tau] (updated)."""
+        st = np.ascontiguousarray(state, np.float64)
+        p = tg_cosmo_params(H0, omega_m, omega_lambda)
+        check("tg_leapfrog_cosmo", lib.tg_leapfrog_cosmo(self.h, C.byref(p), st.ctypes.data, float(dt), int(n_steps),
+                                                         _stream(stream)))
+        return st
+
     def energy(self, stream=None) -> dict:
         out = np.zeros(5)
         check("tg_energy", lib.tg_energy(self.h, out.ctypes.data, _stream(stream)))
@@ -294,6 +303,16 @@ class GravityBatch:
         g = np.zeros((self.n, 3), np.float32)
         check("tg_batch_get_forces", lib.tg_batch_get_forces(self.h, phi.ctypes.data, g.ctypes.data, TG_HOST))
         return phi, g
+
+
+def cosmo_kdk(state, dt, H0, omega_m=0.3, omega_lambda=0.7):
+    """One KDK step's cosmological factors (src/cosmo.cpp:50-106,187-218):
+    returns (new state [a, da/dt, tau], [kick1, drift, kick2])."""
+    st = np.array(state, np.float64)
+    f = np.zeros(3)
+    p = tg_cosmo_params(H0, omega_m, omega_lambda)
+    check("tg_cosmo_kdk", lib.tg_cosmo_kdk(C.byref(p), st.ctypes.data, float(dt), f.ctypes.data))
+    return st, f
 
 
 def device_fp32_peak(device=0) -> float:
