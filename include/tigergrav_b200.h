@@ -178,6 +178,16 @@ typedef struct tg_cosmo_params {
 int tg_cosmo_kdk(const tg_cosmo_params *p, double *state, double dt, double *factors);
 int tg_leapfrog_cosmo(tg_solver *s, const tg_cosmo_params *p, double *state, double dt, int n_steps, void *stream);
 
+/* ---- initial conditions -----------------------------------------------------
+ * load_header / load_particles (src/load.cpp:13-96): an N-GenIC / Gadget-1 file
+ * (256-byte io_header_1, then positions and velocities of type-1 particles).
+ * header (8 doubles, may be NULL): npart[1], redshift, mass[1], Omega0,
+ * OmegaLambda, HubbleParam, BoxSize, time.  With x == NULL only the header and
+ * *n_out are read; otherwise x (n x 3 int32, fixed point) and v (n x 3 float,
+ * may be NULL) are filled as the reference does (shift by 0.5 N^(-1/3), wrap,
+ * double_to_pos; v * a^1.5); capacity < n gives TG_ERR_SIZE.  Host only. */
+int tg_load_gadget1(const char *path, double *header, int32_t *x, float *v, int64_t capacity, int64_t *n_out);
+
 /* ---- batches of independent boxes ---------------------------------------
  * No counterpart in the reference (one box per run).  nboxes periodic unit
  * boxes, box b with counts[b] particles, its own m = 1/counts[b] and

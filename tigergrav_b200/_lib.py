@@ -47,7 +47,7 @@ EXPORTS = [
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
-    "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo",
+    "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo", "tg_load_gadget1",
 ]
 
 
@@ -113,6 +113,7 @@ def _load():
     L.tg_batch_get_forces.argtypes = [vp, vp, vp, i32]
     L.tg_cosmo_kdk.argtypes = [P(tg_cosmo_params), vp, d, vp]
     L.tg_leapfrog_cosmo.argtypes = [vp, P(tg_cosmo_params), vp, d, i32, vp]
+    L.tg_load_gadget1.argtypes = [C.c_char_p, vp, vp, vp, i64, P(i64)]
     return L
 
 

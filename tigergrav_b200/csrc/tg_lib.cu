@@ -8,4 +8,5 @@
 #include "tg_capi.cu"
 #include "tg_batch.cu"
 #include "tg_cosmo.cu"
+#include "tg_load.cu"
 #include "tg_noalloc.cu"

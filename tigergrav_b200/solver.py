@@ -315,6 +315,22 @@ def cosmo_kdk(state, dt, H0, omega_m=0.3, omega_lambda=0.7):
     return st, f
 
 
+def load_gadget1(path):
+    """N-GenIC / Gadget-1 initial conditions as the reference loads them
+    (src/load.cpp:34-96): (header dict, x int32 (n,3) fixed point, v float32 (n,3))."""
+    hdr = np.zeros(8)
+    n = C.c_int64(0)
+    check("tg_load_gadget1", lib.tg_load_gadget1(str(path).encode(), hdr.ctypes.data, None, None, 0, C.byref(n)))
+    x = np.zeros((n.value, 3), np.int32)
+    v = np.zeros((n.value, 3), np.float32)
+    check("tg_load_gadget1", lib.tg_load_gadget1(str(path).encode(), hdr.ctypes.data, x.ctypes.data, v.ctypes.data,
+                                                 n.value, C.byref(n)))
+    keys = ("npart", "redshift", "mass", "omega_m", "omega_lambda", "hubble_param", "box_size", "time")
+    h = dict(zip(keys, hdr.tolist()))
+    h["npart"] = int(h["npart"])
+    return h, x, v
+
+
 def device_fp32_peak(device=0) -> float:
     """Measured FP32 FMA throughput of the device in TFLOP/s."""
     t = C.c_double(0)
