@@ -188,6 +188,27 @@ int tg_leapfrog_cosmo(tg_solver *s, const tg_cosmo_params *p, double *state, dou
  * double_to_pos; v * a^1.5); capacity < n gives TG_ERR_SIZE.  Host only. */
 int tg_load_gadget1(const char *path, double *header, int32_t *x, float *v, int64_t capacity, int64_t *n_out);
 
+/* ---- friends-of-friends groups ----------------------------------------------
+ * tree::find_groups + part_vect_find_groups (src/tree.cpp:637-759,
+ * src/part_vect.cpp:85-124) and the group statistics of src/groups.cpp:124-226.
+ * tg_find_groups: friends are particle pairs whose squared fixed-point
+ * separation (int32 difference: nearest image) is below
+ * ((uint64)(link_len n^(-1/3) (2^32-1)))^2 and non-zero; groups are the
+ * connected components.  group (n int64, caller order, host or device per
+ * where, may be NULL) receives each particle's group id -- the smallest caller
+ * index in its group -- or -1 (the reference's DEFAULT_GROUP) for a particle
+ * without friends; *ngroups (may be NULL) the number of groups.  Builds the
+ * tree and multipoles when the handle has none; link_len n^(-1/3) must lie in
+ * (0, 0.5).  Without ewald the separation is the plain difference.
+ * tg_group_catalog: statistics of the groups of the last tg_find_groups on the
+ * current tree (TG_ERR_STATE otherwise), ids ascending, 14 doubles per group:
+ * id, N, centre x[3] (nearest-image mean, in [0,1)), mean v/a [3], velocity
+ * dispersion [3] (rms of v/a - mean per axis), rmax, rc (median radius,
+ * element N/2 of the sorted radii a |x - centre|), 0.  a: scale factor.  With
+ * out == NULL only *ngroups is set; capacity < ngroups gives TG_ERR_SIZE. */
+int tg_find_groups(tg_solver *s, double link_len, int64_t *group, int64_t *ngroups, int where, void *stream);
+int tg_group_catalog(tg_solver *s, double a, double *out, int64_t capacity, int64_t *ngroups, void *stream);
+
 /* ---- batches of independent boxes ---------------------------------------
  * No counterpart in the reference (one box per run).  nboxes periodic unit
  * boxes, box b with counts[b] particles, its own m = 1/counts[b] and

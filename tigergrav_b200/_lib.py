@@ -48,6 +48,7 @@ EXPORTS = [
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
     "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo", "tg_load_gadget1",
+    "tg_find_groups", "tg_group_catalog",
 ]
 
 
@@ -114,6 +115,8 @@ def _load():
     L.tg_cosmo_kdk.argtypes = [P(tg_cosmo_params), vp, d, vp]
     L.tg_leapfrog_cosmo.argtypes = [vp, P(tg_cosmo_params), vp, d, i32, vp]
     L.tg_load_gadget1.argtypes = [C.c_char_p, vp, vp, vp, i64, P(i64)]
+    L.tg_find_groups.argtypes = [vp, d, vp, P(i64), i32, vp]
+    L.tg_group_catalog.argtypes = [vp, d, vp, i64, P(i64), vp]
     return L
 
 

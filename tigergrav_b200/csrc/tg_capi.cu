@@ -316,6 +316,9 @@ int tg_destroy(tg_solver *s) {
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part);
     release(S.ck_x); release(S.ck_v); release(S.adj_x); release(S.adj_v); release(S.tid_u); release(S.tid_o);
     release(S.tid_U); release(S.tid_V);
+    release(S.fof_P); release(S.fof_leaves); release(S.fof_key); release(S.fof_mem); release(S.fof_runs);
+    release(S.fof_gmin); release(S.fof_group); release(S.fof_has); release(S.fof_pairs); release(S.fof_radii);
+    release(S.fof_stats);
     if (S.h_err) cudaFreeHost(S.h_err);
     if (S.h_cnt) cudaFreeHost(S.h_cnt);
     if (S.h_stage) cudaFreeHost(S.h_stage);

@@ -9,4 +9,5 @@
 #include "tg_batch.cu"
 #include "tg_cosmo.cu"
 #include "tg_load.cu"
+#include "tg_fof.cu"
 #include "tg_noalloc.cu"

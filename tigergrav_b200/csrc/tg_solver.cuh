@@ -125,6 +125,16 @@ struct Solver {
     DevBuf<double2> ew_Pd;
     bool have_tables = false;
 
+    /* friends-of-friends (sorted order unless noted) */
+    DevBuf<int32_t> fof_P, fof_leaves, fof_key, fof_mem, fof_runs;
+    DevBuf<int64_t> fof_gmin, fof_group; /* fof_group: caller order */
+    DevBuf<uint8_t> fof_has;
+    DevBuf<int2> fof_pairs;
+    DevBuf<float> fof_radii;
+    DevBuf<double> fof_stats;
+    int64_t fof_ngroups = 0, fof_npairs = 0;
+    double fof_link = 0.0; /* linking length of the groups held, 0: none for this tree */
+
     /* events for phase timing */
     cudaEvent_t ev[8];
     bool have_events = false;

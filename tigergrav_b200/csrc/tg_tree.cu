@@ -194,6 +194,7 @@ int tree_build(Solver &S, cudaStream_t st) {
     S.depth = L;
     S.nnodes = S.level_off.back();
     S.have_tree = true;
+    S.fof_link = 0.0;
     S.have_multipoles = S.have_lists = S.have_forces = false;
     return TG_OK;
 }

@@ -72,6 +72,41 @@ def clustered(nside: int, seed: int = 2, rms: float = 0.5) -> np.ndarray:
     return double_to_pos(X)
 
 
+def halos(n: int, seed: int = 5, frac: float = 0.6, nmin: int = 10, core: float = 0.1) -> np.ndarray:
+    """A group-finding workload: frac of the n particles in Plummer spheres
+    (sizes from a Pareto law, at least nmin, at most n/50; scale radius
+    core n^(-1/3) N_h^(1/3), cut at 10 scale radii) at uniform random centres,
+    the rest uniform; caller order shuffled.  The displaced-lattice workload
+    above has no pairs closer than a fifth of the mean spacing, so it holds no
+    friends-of-friends groups."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    want = int(frac * n)
+    sizes = []
+    tot = 0
+    cap = max(nmin, n // 50)
+    while tot < want:
+        k = int(min(cap, nmin * (1.0 + rng.pareto(1.0))))
+        k = min(k, want - tot)
+        sizes.append(k)
+        tot += k
+    sizes = np.array(sizes, np.int64)
+    nh = len(sizes)
+    hid = np.repeat(np.arange(nh), sizes)
+    centre = rng.random((nh, 3))
+    a = core * n ** (-1.0 / 3.0) * sizes.astype(np.float64) ** (1.0 / 3.0)
+    umax = 1000.0 / 101.0 ** 1.5  # enclosed fraction of a Plummer sphere inside 10 a
+    u = rng.random(tot) * umax
+    r = a[hid] / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    d = rng.standard_normal((tot, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    X = np.empty((n, 3))
+    X[:tot] = centre[hid] + r[:, None] * d
+    X[tot:] = rng.random((n - tot, 3))
+    X = np.mod(X[rng.permutation(n)], 1.0)
+    X[X >= 1.0] = 0.0
+    return double_to_pos(X)
+
+
 def samples(n: int, count: int = 4096, seed: int = 3) -> np.ndarray:
     """Seeded sample of particle indices for error measurement."""
     rng = np.random.Generator(np.random.PCG64(seed))

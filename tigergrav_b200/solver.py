@@ -182,6 +182,42 @@ class GravitySolver:
         check("tg_tidal", lib.tg_tidal(self.h, u.ctypes.data, out.ctypes.data, TG_HOST, _stream(stream)))
         return out
 
+    def find_groups(self, link_len=0.2, stream=None):
+        """Friends-of-friends groups (tree::find_groups, src/tree.cpp:637-759;
+        the friend test of src/part_vect.cpp:85-124): per caller index the
+        group id (the smallest caller index in the group) or -1 for a particle
+        without friends.  link_len is in mean interparticle spacings."""
+        g = np.zeros(self.n, np.int64)
+        ng = C.c_int64(0)
+        check("tg_find_groups", lib.tg_find_groups(self.h, float(link_len), g.ctypes.data, C.byref(ng), TG_HOST,
+                                                   _stream(stream)))
+        return g
+
+    def group_catalog(self, a=1.0, stream=None) -> dict:
+        """Statistics of the groups of the last find_groups (src/groups.cpp:124-226),
+        ids ascending: id, N, x (n,3), v (n,3), dv (n,3), rmax, rc."""
+        ng = C.c_int64(0)
+        check("tg_group_catalog", lib.tg_group_catalog(self.h, float(a), None, 0, C.byref(ng), _stream(stream)))
+        out = np.zeros((max(ng.value, 1), 14))
+        check("tg_group_catalog", lib.tg_group_catalog(self.h, float(a), out.ctypes.data, ng.value, C.byref(ng),
+                                                       _stream(stream)))
+        out = out[:ng.value]
+        return dict(id=out[:, 0].astype(np.int64), N=out[:, 1].astype(np.int64), x=out[:, 2:5], v=out[:, 5:8],
+                    dv=out[:, 8:11], rmax=out[:, 11], rc=out[:, 12])
+
+    def groups_output(self, path, a=1.0, min_size=10, stream=None):
+        """The group file of groups_output (src/groups.cpp:78-100): one line
+        per group of at least min_size members: id, N, rmax, rc, |v|, |dv|."""
+        c = self.group_catalog(a, stream)
+        with open(path, "wt") as fp:
+            keep = np.nonzero(c["N"] >= min_size)[0]
+            for k in keep:
+                fp.write("%16li %5i %12e %12e %12e %12e\n" % (c["id"][k], c["N"][k], c["rmax"][k], c["rc"][k],
+                                                             np.linalg.norm(c["v"][k]), np.linalg.norm(c["dv"][k])))
+            if len(keep) == 0:
+                fp.write("No groups\n")
+        return len(keep)
+
     def leapfrog_cosmo(self, dt, n_steps, state, H0, omega_m=0.3, omega_lambda=0.7, stream=None):
         """n_steps comoving KDK steps with the cosmological factors; state = [a, da/dt, tau] (updated)."""
         st = np.ascontiguousarray(state, np.float64)
