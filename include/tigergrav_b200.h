@@ -207,6 +207,39 @@ int tg_load_gadget1(const char *path, double *header, int32_t *x, float *v, int6
  * element N/2 of the sorted radii a |x - centre|), 0.  a: scale factor.  With
  * out == NULL only *ngroups is set; capacity < ngroups gives TG_ERR_SIZE. */
 int tg_find_groups(tg_solver *s, double link_len, int64_t *group, int64_t *ngroups, int where, void *stream);
+
+/* ---- hierarchical (rung) time steps ------------------------------------------
+ * tigergrav/time.hpp:12-48, the main loop step (src/main.cpp:266-313) and the
+ * rung kick of part_vect_kick (src/part_vect.cpp:340-381).  Rung r has step
+ * t_max / 2^r; the integer time itime counts t_max / 2^31.  tg_rung_step with
+ * max_rung < 0 (a fresh state: itime 0) does the first solve and kick; each
+ * later call drifts all particles by t_max / 2^max_rung, advances itime by
+ * 2^(31 - max_rung), solves gravity with only the particles of rung >=
+ * min_rung(itime) as sinks (all particles when all_forces; the reference's
+ * do_out) and kicks those: half a step of the old rung (not on rung 0), new
+ * rung from dt = min(dt_max, eta sqrt(soft_len / 2.8 / |g G|)) (at least
+ * min_rung), half a step of the new rung; stored rung max(rung, old - 1, 1).
+ * max_rung returns the largest new rung of the active particles.  Non-
+ * cosmological; the second half kick is 0.5 dt (the reference's periodic
+ * runs zero it by testing opts.ewald for opts.cosmic).  Forces of inactive
+ * particles are not evaluated, so tg_get_forces answers TG_ERR_STATE after a
+ * step without all_forces.  Rungs start at 0 (tg_set_particles) and travel
+ * with the particles; tg_get_rungs reads them in caller order (n int8). */
+typedef struct {
+    double t_max;  /* options::t_max */
+    double dt_max; /* options::dt_max */
+    double eta;    /* options::eta */
+} tg_rung_params;
+typedef struct {
+    uint32_t itime;     /* integer time, 2^31 == t_max */
+    int32_t max_rung;   /* largest rung of the last kick; -1 before the first step */
+    int32_t min_rung;   /* lowest active rung of the last step */
+    int32_t reserved;
+    int64_t num_active; /* particles kicked by the last step */
+    double t;           /* itime in units of time */
+} tg_rung_state;
+int tg_rung_step(tg_solver *s, const tg_rung_params *p, tg_rung_state *state, int all_forces, void *stream);
+int tg_get_rungs(tg_solver *s, int8_t *rung, int where, void *stream);
 int tg_group_catalog(tg_solver *s, double a, double *out, int64_t capacity, int64_t *ngroups, void *stream);
 
 /* ---- batches of independent boxes ---------------------------------------

@@ -154,3 +154,41 @@ def test_fof_edges(tmp_path):
         k = s.groups_output(tmp_path / "groups.0.0.dat", min_size=10)
         lines = (tmp_path / "groups.0.0.dat").read_text().splitlines()
     assert k == 4 and len(lines) == 4 and int(lines[0].split()[1]) >= 10
+
+
+@pytest.mark.gpu
+def test_fof_full_size_partition_and_catalog():
+    """128^3 particles (the bench's size): the partition equals the oracle's;
+    the catalogue covers every grouped particle once, ids ascending."""
+    from tigergrav_b200 import ics
+    from tigergrav_b200.solver import GravitySolver
+    x = ics.halos(128 ** 3)
+    ref = ofof.groups(x, 0.2)
+    with GravitySolver(len(x), theta=0.7) as s:
+        s.set_particles(x)
+        g = s.find_groups(0.2)
+        c = s.group_catalog(1.0)
+    assert np.array_equal(g, ref)
+    ids, cnt = np.unique(ref[ref >= 0], return_counts=True)
+    assert np.array_equal(c["id"], ids) and np.array_equal(c["N"], cnt)
+    assert (c["rc"] <= c["rmax"]).all() and (c["rc"] >= 0).all()
+
+
+@pytest.mark.gpu
+def test_fof_catalog_64cubed_matches_oracle():
+    from tigergrav_b200 import ics
+    from tigergrav_b200.solver import GravitySolver
+    x = ics.halos(64 ** 3, seed=6)
+    v = np.random.default_rng(2).standard_normal((len(x), 3)).astype(np.float32)
+    g_ref = ofof.groups(x, 0.2)
+    ref = ofof.catalog(x, v, g_ref, a=0.5)
+    with GravitySolver(len(x), theta=0.7) as s:
+        s.set_particles(x, v)
+        assert np.array_equal(s.find_groups(0.2), g_ref)
+        c = s.group_catalog(0.5)
+    assert np.array_equal(c["id"], ref["id"]) and np.array_equal(c["N"], ref["N"])
+    dx = np.abs(c["x"] - ref["x"])
+    assert np.minimum(dx, 1.0 - dx).max() < 1e-9
+    assert np.allclose(c["dv"], ref["dv"], rtol=1e-5, atol=1e-6)
+    assert np.allclose(c["rmax"], ref["rmax"], rtol=1e-5, atol=1e-9)
+    assert np.allclose(c["rc"], ref["rc"], rtol=1e-5, atol=1e-9)

@@ -1,0 +1,123 @@
+"""Hierarchical (rung) time steps (tg_rung_step, tg_get_rungs).
+
+CPU: the oracle's integer time line against values that follow from
+tigergrav/time.hpp:12-48 by hand, and its kick rules.  GPU: K rung steps of
+the library against the oracle's stepper driven by the library's own full
+solve (every particle a sink) and the oracle's drift: positions, velocities
+and rungs bit-identical, which also shows that the walk restricted to active
+sinks gives the active particles exactly the forces of a full solve."""
+import numpy as np
+import pytest
+
+import rungs as orung
+
+
+def test_time_line_by_hand():
+    assert orung.min_rung(0) == 0
+    assert orung.min_rung(1 << 30) == 1
+    assert orung.min_rung(3 << 28) == 3
+    assert orung.min_rung(1) == 31
+    assert orung.inc(0, 3) == 1 << 28 and orung.inc(1 << 28, 3) == 1 << 29
+    assert orung.inc(0, 0) == 1 << 31
+    assert orung.time_to_double(1 << 30, 2.0) == 1.0
+    assert orung.rung_to_dt(1.0, 4) == 1.0 / 16
+    # the smallest rung whose step is <= dt
+    assert orung.dt_to_rung(1.0, np.array([1.0, 0.5, 0.49, 0.25, 1e-3])).tolist() == [0, 1, 2, 2, 10]
+    with pytest.raises(ValueError):
+        orung.dt_to_rung(1.0, np.array([1e-12]))
+
+
+def test_kick_rules():
+    t_max, h, eta = 1.0, 1e-3, 0.1
+    v = np.zeros((4, 3), np.float32)
+    rung = np.array([0, 3, 8, 2], np.int8)
+    g = np.array([[1e3, 0, 0], [1e-6, 0, 0], [1e-6, 0, 0], [1.0, 0, 0]], np.float32)
+    mr = orung.kick(v, rung, g, 2, t_max, 0.5, eta, h)
+    # particle 0 is below min_rung 2: untouched
+    assert rung[0] == 0 and (v[0] == 0).all()
+    # particle 1: tiny force -> dt_max -> rung 1, raised to min_rung 2; stored max(2, 3 - 1, 1)
+    assert rung[1] == 2
+    want = np.float32(np.float32(1e-6) * np.float32(0.5 / 8)) + np.float32(1e-6) * np.float32(0.5 / 4)
+    assert v[1, 0] == want
+    # particle 2: the stored rung drops by one per kick at most, though its new rung is 2
+    assert rung[2] == 7
+    # particle 3: dt = eta sqrt(h / 2.8) = 1.89e-3 -> rung 10 (2^-10 <= dt < 2^-9)
+    assert rung[3] == 10
+    assert mr == 10
+
+
+# ---------------------------------------------------------------- GPU -------
+
+T_MAX, DT_MAX, ETA = 1.0 / 64, 1.0 / 128, 0.2
+
+
+def _stepper(x, soft_len, theta=0.7):
+    import oracle
+    from tigergrav_b200.solver import GravitySolver
+    n = len(x)
+    full = GravitySolver(n, theta=theta)
+    o = oracle.Oracle(theta=theta)
+
+    def forces(xx, vv):
+        full.set_particles(xx, vv).solve_gravity()
+        return full.get_forces(dtype=np.float32)[1]
+
+    def drift(xx, vv, dt):
+        o.set_particles(xx, vv)
+        o.drift(dt)
+        return o.particles()[0]
+
+    return orung.Stepper(x, np.zeros((n, 3), np.float32), forces, drift, T_MAX, DT_MAX, ETA, soft_len), full
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_rung_steps_match_oracle(precision):
+    from tigergrav_b200 import ics
+    from tigergrav_b200.solver import GravitySolver
+    x = ics.halos(4096, seed=3)
+    n = len(x)
+    with GravitySolver(n, theta=0.7, precision=precision) as s:
+        h = s.params.soft_len
+        ref, full = _stepper(x, h)
+        if precision == "f64":
+            full.close()
+            full = GravitySolver(n, theta=0.7, precision="f64")
+            ref.forces = lambda xx, vv: full.set_particles(xx, vv).solve_gravity().get_forces(dtype=np.float32)[1]
+        s.set_particles(x)
+        state = None
+        actives = []
+        for k in range(12):
+            state = s.rung_step(state, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+            want = ref.step()
+            actives.append(state["num_active"])
+            assert state == pytest.approx(want), k
+            xs, vs = s.get_particles()
+            assert np.array_equal(s.rungs(), ref.rung), k
+            assert np.array_equal(xs, ref.x), k
+            assert np.array_equal(vs, ref.v), k
+        full.close()
+    assert len(set(np.bincount(ref.rung).nonzero()[0])) >= 3  # several rungs in use
+    assert min(actives) < n // 2  # some steps had few sinks
+
+
+@pytest.mark.gpu
+def test_rung_step_forces_state():
+    from tigergrav_b200 import _lib, ics
+    from tigergrav_b200.solver import GravitySolver
+    x = ics.halos(4096, seed=3)
+    with GravitySolver(len(x), theta=0.7) as s, GravitySolver(len(x), theta=0.7) as full:
+        s.set_particles(x)
+        st = s.rung_step(None, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+        st = s.rung_step(st, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+        if st["num_active"] < len(x):
+            with pytest.raises(_lib.TGError):
+                s.get_forces()
+        # with all_forces every particle is a sink: forces equal a full solve's
+        st = s.rung_step(st, t_max=T_MAX, dt_max=DT_MAX, eta=ETA, all_forces=True)
+        xs, vs = s.get_particles()
+        full.set_particles(xs, vs).solve_gravity()
+        assert np.array_equal(s.get_forces(dtype=np.float32)[1], full.get_forces(dtype=np.float32)[1])
+        # a step far below t_max / 2^30 is refused
+        with pytest.raises(_lib.TGError):
+            s.rung_step(st, t_max=T_MAX, dt_max=T_MAX * 1e-12, eta=ETA)

@@ -29,6 +29,15 @@ class tg_cosmo_params(C.Structure):
     _fields_ = [("H0", C.c_double), ("omega_m", C.c_double), ("omega_lambda", C.c_double)]
 
 
+class tg_rung_params(C.Structure):
+    _fields_ = [("t_max", C.c_double), ("dt_max", C.c_double), ("eta", C.c_double)]
+
+
+class tg_rung_state(C.Structure):
+    _fields_ = [("itime", C.c_uint32), ("max_rung", C.c_int32), ("min_rung", C.c_int32), ("reserved", C.c_int32),
+                ("num_active", C.c_int64), ("t", C.c_double)]
+
+
 class tg_stats(C.Structure):
     _fields_ = [("n", C.c_int64), ("nodes", C.c_int64), ("leaves", C.c_int64), ("depth", C.c_int32),
                 ("walk_retries", C.c_int32), ("ref_stats", C.c_uint64 * 6), ("counts", C.c_uint64 * 8),
@@ -48,7 +57,7 @@ EXPORTS = [
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
     "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo", "tg_load_gadget1",
-    "tg_find_groups", "tg_group_catalog",
+    "tg_find_groups", "tg_group_catalog", "tg_rung_step", "tg_get_rungs",
 ]
 
 
@@ -117,6 +126,8 @@ def _load():
     L.tg_load_gadget1.argtypes = [C.c_char_p, vp, vp, vp, i64, P(i64)]
     L.tg_find_groups.argtypes = [vp, d, vp, P(i64), i32, vp]
     L.tg_group_catalog.argtypes = [vp, d, vp, i64, P(i64), vp]
+    L.tg_rung_step.argtypes = [vp, P(tg_rung_params), P(tg_rung_state), i32, vp]
+    L.tg_get_rungs.argtypes = [vp, vp, i32, vp]
     return L
 
 

@@ -319,6 +319,7 @@ int tg_destroy(tg_solver *s) {
     release(S.fof_P); release(S.fof_leaves); release(S.fof_key); release(S.fof_mem); release(S.fof_runs);
     release(S.fof_gmin); release(S.fof_group); release(S.fof_has); release(S.fof_pairs); release(S.fof_radii);
     release(S.fof_stats);
+    release(S.rung_flag); release(S.rung_scan); release(S.rung_nact); release(S.rung_out);
     if (S.h_err) cudaFreeHost(S.h_err);
     if (S.h_cnt) cudaFreeHost(S.h_cnt);
     if (S.h_stage) cudaFreeHost(S.h_stage);

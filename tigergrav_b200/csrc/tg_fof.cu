@@ -21,13 +21,14 @@
  *   k_fof_link    one warp per leaf pair tests its particle pairs and joins
  *                 friends in a lock-free union-find: parents only ever point
  *                 to smaller sorted indices, roots are hooked with atomicCAS;
- *   k_fof_roots   every particle points at its root, and each root gets the
- *                 smallest caller index of its group -- the group id reported
- *                 (the reference labels by its own storage order).
+ *   k_fof_roots   the root of every particle (a read-only walk up the
+ *                 parents), and at each root the smallest caller index of its
+ *                 group -- the group id reported (the reference labels by its
+ *                 own storage order).
  * Catalogue: members sorted by root (CUB radix sort), one block per group sums
  * the offsets from the root particle (nearest image) and the velocities in a
- * fixed order, then radii a |x - centre| and velocity dispersion; the median
- * radius comes from a CUB segmented sort of the radii.
+ * fixed order, then radii a |x - centre|, velocity dispersion and the median
+ * radius (a radix select inside the block).
  */
 #include <algorithm>
 #include <cmath>
@@ -180,24 +181,31 @@ __global__ void k_fof_link(int64_t npairs, const int2 *__restrict__ pairs, const
     }
 }
 
-/* every particle at its root; each root keeps the smallest caller index of its group */
-__global__ void k_fof_roots(int64_t n, int32_t *P, const int4 *__restrict__ pos, int64_t *__restrict__ gmin) {
+/* root of every particle (into R), and at each root the smallest caller index of its group.
+ * P is only read here: path compression while other threads take R from the
+ * same paths could leave a particle pointing at an inner node. */
+__global__ void k_fof_roots(int64_t n, const int32_t *__restrict__ P, const int4 *__restrict__ pos,
+                            int32_t *__restrict__ R, int64_t *__restrict__ gmin) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int32_t r = fof_find(P, (int32_t)i);
-    P[i] = r;
-    atomicMin((unsigned long long *)&gmin[r], (unsigned long long)pos[i].w);
+    int32_t x = (int32_t)i, p = P[x];
+    while (p != x) { /* parents strictly decrease: ends within n steps */
+        x = p;
+        p = P[x];
+    }
+    R[i] = x;
+    atomicMin((unsigned long long *)&gmin[x], (unsigned long long)pos[i].w);
 }
 
 /* group id per caller index (-1: no friend); sort keys for the catalogue; group count */
-__global__ void k_fof_out(int64_t n, const int32_t *__restrict__ P, const int4 *__restrict__ pos,
+__global__ void k_fof_out(int64_t n, const int32_t *__restrict__ R, const int4 *__restrict__ pos,
                           const int64_t *__restrict__ gmin, const uint8_t *__restrict__ has_friend,
                           int64_t *__restrict__ group, int32_t *__restrict__ key, int32_t *__restrict__ member,
                           unsigned long long *__restrict__ cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const bool f = has_friend[i] != 0;
-    const int32_t r = P[i];
+    const int32_t r = R[i];
     group[pos[i].w] = f ? gmin[r] : -1;
     key[i] = f ? r : 0x7fffffff;
     member[i] = (int32_t)i;
@@ -208,21 +216,34 @@ __global__ void k_fof_out(int64_t n, const int32_t *__restrict__ P, const int4 *
  * One block per group: centre = root position + mean nearest-image offset
  * (wrapped into [0,1)), mean velocity / a, then per member the radius
  * a |nearest image (x - centre)| (src/groups.cpp:184-190, as float), its
- * maximum, and the velocity dispersion sqrt(mean (v/a - <v/a>)^2) per axis.
- * All sums run in a fixed order: deterministic.
- * stats per group (12 doubles): x[3], v[3], dv[3], rmax, N, id
+ * maximum, the velocity dispersion sqrt(mean (v/a - <v/a>)^2) per axis, and
+ * the median radius, element N/2 of the sorted radii (src/groups.cpp:217-221),
+ * by a radix select over the float bit patterns (radii are >= 0, so their
+ * bits order like their values): four 8-bit histogram passes in shared
+ * memory.  All sums run in a fixed order: deterministic.
+ * stats per group (13 doubles): x[3], v[3], dv[3], rmax, N, id, rc
  */
-__global__ void __launch_bounds__(FOF_TPB) k_group_stats(const int32_t *__restrict__ roots, const int32_t *__restrict__ off,
+static_assert(FOF_TPB == 256, "one histogram bin per thread");
+__global__ void __launch_bounds__(FOF_TPB) k_group_stats(int64_t n, const int32_t *__restrict__ roots,
+                                                         const int32_t *__restrict__ off,
                                                          const int32_t *__restrict__ cnt, const int32_t *__restrict__ member,
                                                          const int4 *__restrict__ pos, const float4 *__restrict__ vel,
                                                          const int64_t *__restrict__ gmin, double a, int periodic,
-                                                         float *__restrict__ radii, double *__restrict__ stats) {
+                                                         float *radii, double *__restrict__ stats,
+                                                         uint32_t *__restrict__ err) {
     const int g = blockIdx.x;
     const int32_t b = off[g], N = cnt[g];
-    const int4 anchor = pos[roots[g]];
-    __shared__ double red[7][FOF_TPB];
+    const int32_t root = roots[g];
+    if (b < 0 || N <= 0 || (int64_t)b + N > n || root < 0 || root >= n) { /* cannot happen: checked, not trusted */
+        if (threadIdx.x == 0) atomicOr(err, 16u);
+        return;
+    }
+    const int4 anchor = pos[root];
+    __shared__ double red[6][FOF_TPB];
     __shared__ double cen[6];
-    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    __shared__ unsigned int hist[256];
+    __shared__ unsigned int sel_prefix, sel_k;
+    double s[6] = {0, 0, 0, 0, 0, 0};
     for (int32_t j = threadIdx.x; j < N; j += FOF_TPB) {
         const int32_t i = member[b + j];
         const int4 p = pos[i];
@@ -250,9 +271,11 @@ __global__ void __launch_bounds__(FOF_TPB) k_group_stats(const int32_t *__restri
             cen[d] = c;
             cen[3 + d] = red[3 + d][0] / N / a;
         }
+        sel_prefix = 0u;
+        sel_k = (unsigned int)(N / 2);
     }
     __syncthreads();
-    for (int k = 0; k < 7; k++) s[k] = 0.0;
+    for (int k = 0; k < 4; k++) s[k] = 0.0;
     for (int32_t j = threadIdx.x; j < N; j += FOF_TPB) {
         const int32_t i = member[b + j];
         const int4 p = pos[i];
@@ -271,6 +294,7 @@ __global__ void __launch_bounds__(FOF_TPB) k_group_stats(const int32_t *__restri
         radii[b + j] = r;
         s[3] = fmax(s[3], (double)r);
     }
+    __syncthreads(); /* radii[] complete and red[] free */
     for (int k = 0; k < 4; k++) red[k][threadIdx.x] = s[k];
     __syncthreads();
     for (int h = FOF_TPB / 2; h > 0; h >>= 1) {
@@ -280,8 +304,32 @@ __global__ void __launch_bounds__(FOF_TPB) k_group_stats(const int32_t *__restri
         }
         __syncthreads();
     }
+    /* element N/2 of the sorted radii: radix select, 8 bits a pass from the top */
+    unsigned int mask = 0u;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        hist[threadIdx.x] = 0u;
+        __syncthreads();
+        const unsigned int pre = sel_prefix;
+        for (int32_t j = threadIdx.x; j < N; j += FOF_TPB) {
+            const unsigned int u = __float_as_uint(radii[b + j]);
+            if ((u & mask) == pre) atomicAdd(&hist[(u >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int k = sel_k, c = 0u;
+            int bin = 0;
+            for (; bin < 255; bin++) {
+                if (c + hist[bin] > k) break;
+                c += hist[bin];
+            }
+            sel_k = k - c;
+            sel_prefix = pre | ((unsigned int)bin << shift);
+        }
+        mask |= 255u << shift;
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
-        double *o = stats + 12 * (int64_t)g;
+        double *o = stats + 13 * (int64_t)g;
         for (int d = 0; d < 3; d++) {
             o[d] = cen[d];
             o[3 + d] = cen[3 + d];
@@ -289,21 +337,9 @@ __global__ void __launch_bounds__(FOF_TPB) k_group_stats(const int32_t *__restri
         }
         o[9] = red[3][0];
         o[10] = N;
-        o[11] = (double)gmin[roots[g]];
+        o[11] = (double)gmin[root];
+        o[12] = (double)__uint_as_float(sel_prefix);
     }
-}
-
-/* group sizes and offsets from the run-length encoding of the sorted keys */
-__global__ void k_group_offsets(int32_t ng, const int32_t *__restrict__ cnt, const int32_t *__restrict__ off,
-                                int32_t *__restrict__ end) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < ng) end[g] = off[g] + cnt[g];
-}
-
-__global__ void k_group_median(int32_t ng, const int32_t *__restrict__ off, const int32_t *__restrict__ cnt,
-                               const float *__restrict__ sorted, double *__restrict__ rc) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < ng) rc[g] = sorted[off[g] + cnt[g] / 2]; /* radii[size / 2], src/groups.cpp:219-221 */
 }
 
 /*
@@ -358,12 +394,13 @@ static int fof_run(Solver &S, double link_len, int64_t *group_dev, int64_t *ngro
                                                                  S.dev_err.p);
         TG_TRY(launched(S));
     }
-    k_fof_roots<<<gn, 256, 0, st>>>(n, S.fof_P.p, S.pos.p, S.fof_gmin.p);
-    TG_TRY(launched(S));
     TG_TRY(ensure(S.fof_key, 2 * n));
     TG_TRY(ensure(S.fof_mem, 2 * n));
+    int32_t *R = S.fof_key.p + n; /* roots; this half of the key buffer is free until the catalogue sorts */
+    k_fof_roots<<<gn, 256, 0, st>>>(n, S.fof_P.p, S.pos.p, R, S.fof_gmin.p);
+    TG_TRY(launched(S));
     TG_CUDA(cudaMemsetAsync(S.dev_cnt.p + 2, 0, sizeof(unsigned long long), st));
-    k_fof_out<<<gn, 256, 0, st>>>(n, S.fof_P.p, S.pos.p, S.fof_gmin.p, S.fof_has.p, group_dev, S.fof_key.p,
+    k_fof_out<<<gn, 256, 0, st>>>(n, R, S.pos.p, S.fof_gmin.p, S.fof_has.p, group_dev, S.fof_key.p,
                                   S.fof_mem.p, S.dev_cnt.p + 2);
     TG_TRY(launched(S));
     uint32_t err = 0;
@@ -393,47 +430,44 @@ static int fof_catalog(Solver &S, double a, std::vector<double> &out, cudaStream
     TG_TRY(ensure(S.cub_tmp, tmp));
     TG_CUDA(cub::DeviceRadixSort::SortPairs(S.cub_tmp.p, tmp, key_in, key_out, mem_in, mem_out, (int)n, 0, 32, st));
     /* runs of equal roots: the groups first (keys < INT_MAX), then at most one run of loners */
-    TG_TRY(ensure(S.fof_runs, 4 * (ng + 2)));
-    int32_t *roots = S.fof_runs.p, *cnt = roots + (ng + 2), *off = cnt + (ng + 2), *end = off + (ng + 2);
+    /* sized for n runs, the most there can be, so the encode never writes past them */
+    TG_TRY(ensure(S.fof_runs, 3 * (n + 1)));
+    int32_t *roots = S.fof_runs.p, *cnt = roots + (n + 1), *off = cnt + (n + 1);
     size_t tmp2 = 0;
     TG_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, tmp2, key_out, roots, cnt, S.dev_cnt.p + 3, (int)n, st));
     TG_TRY(ensure(S.cub_tmp, tmp2));
     TG_CUDA(cub::DeviceRunLengthEncode::Encode(S.cub_tmp.p, tmp2, key_out, roots, cnt, S.dev_cnt.p + 3, (int)n, st));
+    TG_CUDA(cudaMemcpyAsync(S.h_cnt + 3, S.dev_cnt.p + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    const int64_t runs = (int64_t)S.h_cnt[3];
+    if (runs != ng && runs != ng + 1) return TG_ERR_STATE; /* one run per group, plus the loners */
     size_t tmp3 = 0;
     TG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, cnt, off, (int)ng, st));
     TG_TRY(ensure(S.cub_tmp, tmp3));
     TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, tmp3, cnt, off, (int)ng, st));
-    k_group_offsets<<<(int)((ng + 255) / 256), 256, 0, st>>>((int32_t)ng, cnt, off, end);
-    TG_TRY(launched(S));
-    TG_TRY(ensure(S.fof_radii, 2 * n));
+    TG_TRY(ensure(S.fof_radii, n));
     TG_TRY(ensure(S.fof_stats, 13 * ng));
-    k_group_stats<<<(int)ng, FOF_TPB, 0, st>>>(roots, off, cnt, mem_out, S.pos.p, S.vel.p, S.fof_gmin.p, a, periodic,
-                                              S.fof_radii.p, S.fof_stats.p);
+    TG_CUDA(cudaMemsetAsync(S.dev_err.p, 0, sizeof(uint32_t), st));
+    k_group_stats<<<(int)ng, FOF_TPB, 0, st>>>(n, roots, off, cnt, mem_out, S.pos.p, S.vel.p, S.fof_gmin.p, a,
+                                              periodic, S.fof_radii.p, S.fof_stats.p, S.dev_err.p);
     TG_TRY(launched(S));
-    /* members in groups come first in the sorted order, so the segments cover [0, members) */
-    size_t tmp4 = 0;
-    float *rad_out = S.fof_radii.p + n;
-    TG_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp4, S.fof_radii.p, rad_out, (int)n, (int)ng, off, end, st));
-    TG_TRY(ensure(S.cub_tmp, tmp4));
-    TG_CUDA(cub::DeviceSegmentedSort::SortKeys(S.cub_tmp.p, tmp4, S.fof_radii.p, rad_out, (int)n, (int)ng, off, end,
-                                               st));
-    double *rc = S.fof_stats.p + 12 * ng;
-    k_group_median<<<(int)((ng + 255) / 256), 256, 0, st>>>((int32_t)ng, off, cnt, rad_out, rc);
-    TG_TRY(launched(S));
+    uint32_t err = 0;
+    TG_TRY(read_err(S, st, &err));
+    if (err) return TG_ERR_STATE;
     std::vector<double> h(13 * ng);
     TG_CUDA(cudaMemcpyAsync(h.data(), S.fof_stats.p, sizeof(double) * 13 * ng, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
     std::vector<int64_t> order(ng);
     for (int64_t g = 0; g < ng; g++) order[g] = g;
-    std::sort(order.begin(), order.end(), [&](int64_t p, int64_t q) { return h[12 * p + 11] < h[12 * q + 11]; });
+    std::sort(order.begin(), order.end(), [&](int64_t p, int64_t q) { return h[13 * p + 11] < h[13 * q + 11]; });
     for (int64_t k = 0; k < ng; k++) {
-        const double *s = &h[12 * order[k]];
+        const double *s = &h[13 * order[k]];
         double *o = &out[14 * k];
         o[0] = s[11];
         o[1] = s[10];
         for (int d = 0; d < 9; d++) o[2 + d] = s[d];
         o[11] = s[9];
-        o[12] = h[12 * ng + order[k]];
+        o[12] = s[12];
     }
     return TG_OK;
 }

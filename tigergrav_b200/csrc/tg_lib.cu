@@ -10,4 +10,5 @@
 #include "tg_cosmo.cu"
 #include "tg_load.cu"
 #include "tg_fof.cu"
+#include "tg_rung.cu"
 #include "tg_noalloc.cu"

@@ -125,6 +125,11 @@ struct Solver {
     DevBuf<double2> ew_Pd;
     bool have_tables = false;
 
+    /* rung (individual) time steps: the rung lives in vel[i].w */
+    DevBuf<int32_t> rung_flag, rung_scan, rung_nact; /* active flag per particle, its scan, active per node */
+    DevBuf<int8_t> rung_out;                         /* caller-order rungs for tg_get_rungs */
+    const int32_t *walk_nact = nullptr;              /* set during a rung step's walk only */
+
     /* friends-of-friends (sorted order unless noted) */
     DevBuf<int32_t> fof_P, fof_leaves, fof_key, fof_mem, fof_runs;
     DevBuf<int64_t> fof_gmin, fof_group; /* fof_group: caller order */

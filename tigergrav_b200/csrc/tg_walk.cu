@@ -37,6 +37,7 @@ struct WalkParams {
     double h;
     float r_ewald;
     int ewald;
+    const int32_t *nact; /* active particles per node (rung steps); nullptr: every particle is a sink */
 };
 
 constexpr uint32_t OPENED = 0x80000000u;
@@ -205,7 +206,8 @@ __global__ void k_node_stage(WalkParams W, NodeView V, int64_t first, int64_t co
     const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (k >= count) return;
     const int32_t i = (int32_t)(first + k);
-    if (V.pe[i] == V.pb[i]) {
+    /* a node without active particles gets no lists (src/tree.cpp:396): it stays a source only */
+    if (V.pe[i] == V.pb[i] || (W.nact && W.nact[i] == 0)) {
         if (lane == 0) {
             nx_len_d[i] = 0;
             nx_len_e[i] = 0;
@@ -378,10 +380,10 @@ __global__ void k_leaf_drain(WalkParams W, NodeView V, const int32_t *__restrict
 }
 
 __global__ void k_collect_leaves(int64_t nn, const int32_t *pb, const int32_t *pe, const int32_t *child0,
-                                 int32_t *leaves, unsigned long long *count) {
+                                 const int32_t *nact, int32_t *leaves, unsigned long long *count) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
-    if (child0[i] < 0 && pe[i] > pb[i]) {
+    if (child0[i] < 0 && pe[i] > pb[i] && (!nact || nact[i] > 0)) {
         const unsigned long long k = atomicAdd(count, 1ull);
         leaves[k] = (int32_t)i;
     }
@@ -404,6 +406,7 @@ int tree_walk(Solver &S, cudaStream_t st) {
     W.h = S.prm.soft_len;
     W.r_ewald = (float)(2.0 * S.prm.theta * std::pow(1.0e-3 / 8.0, 1.0 / 3.0));
     W.ewald = S.prm.ewald ? 1 : 0;
+    W.nact = S.walk_nact;
     NodeView V{S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p, S.nd_r.p, S.nd_rmax.p};
 
     for (int k = 0; k < NLIST; k++) {
@@ -430,7 +433,7 @@ int tree_walk(Solver &S, cudaStream_t st) {
     TG_CUDA(cudaMemsetAsync(S.pool_top.p, 0, sizeof(unsigned long long) * (NLIST + 4), st));
     {
         const int g = (int)((nn + 255) / 256);
-        k_collect_leaves<<<g, 256, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.idx.p, S.pool_top.p + NLIST + 2);
+        k_collect_leaves<<<g, 256, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.walk_nact, S.idx.p, S.pool_top.p + NLIST + 2);
         TG_TRY(launched(S));
     }
     unsigned long long nleaves_h = 0;

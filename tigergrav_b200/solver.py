@@ -27,7 +27,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import lib, check, tg_params, tg_stats, tg_cosmo_params, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, \
+from ._lib import lib, check, tg_params, tg_stats, tg_cosmo_params, tg_rung_params, tg_rung_state, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, \
     LIST_KINDS
 
 
@@ -217,6 +217,25 @@ class GravitySolver:
             if len(keep) == 0:
                 fp.write("No groups\n")
         return len(keep)
+
+    def rung_step(self, state=None, t_max=1.0, dt_max=None, eta=0.2, all_forces=False, stream=None):
+        """One step of hierarchical (rung) time stepping (src/main.cpp:266-313,
+        src/part_vect.cpp:340-381); state None starts at itime 0.  Returns the
+        new state dict: itime, max_rung, min_rung, num_active, t."""
+        st = tg_rung_state(0, -1, 0, 0, 0, 0.0)
+        if state is not None:
+            st.itime, st.max_rung, st.min_rung = state["itime"], state["max_rung"], state["min_rung"]
+            st.num_active, st.t = state["num_active"], state["t"]
+        p = tg_rung_params(float(t_max), float(t_max if dt_max is None else dt_max), float(eta))
+        check("tg_rung_step", lib.tg_rung_step(self.h, C.byref(p), C.byref(st), int(bool(all_forces)),
+                                               _stream(stream)))
+        return dict(itime=st.itime, max_rung=st.max_rung, min_rung=st.min_rung, num_active=st.num_active, t=st.t)
+
+    def rungs(self, stream=None) -> np.ndarray:
+        """Per-particle rungs in caller order (int8)."""
+        r = np.zeros(self.n, np.int8)
+        check("tg_get_rungs", lib.tg_get_rungs(self.h, r.ctypes.data, TG_HOST, _stream(stream)))
+        return r
 
     def leapfrog_cosmo(self, dt, n_steps, state, H0, omega_m=0.3, omega_lambda=0.7, stream=None):
         """n_steps comoving KDK steps with the cosmological factors; state = [a, da/dt, tau] (updated)."""
