@@ -313,7 +313,7 @@ int tg_destroy(tg_solver *s) {
     }
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
     release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
-    release(S.ew_cnt); release(S.ew_off); release(S.ew_part);
+    release(S.ew_cnt); release(S.ew_off); release(S.ew_part); release(S.ew_nt); release(S.ew_sf); release(S.ew_tpart);
     release(S.ck_x); release(S.ck_v); release(S.adj_x); release(S.adj_v); release(S.tid_u); release(S.tid_o);
     release(S.tid_U); release(S.tid_V);
     release(S.fof_P); release(S.fof_leaves); release(S.fof_key); release(S.fof_mem); release(S.fof_runs);

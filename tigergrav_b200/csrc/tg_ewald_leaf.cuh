@@ -37,12 +37,13 @@ __global__ void k_ewald_count(const int32_t *__restrict__ leaves, int32_t nleave
 }
 
 /* one chunk: PP_E entries [k EW_KPP, ...) or PC_E entries [(k - npp) EW_KPC, ...) of its leaf */
-template <class T>
+template <class T, bool SEP>
 __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
                                                     const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
                                                     const int32_t *__restrict__ pe, const MSrc *__restrict__ ms,
                                                     const int4 *__restrict__ pos, ListView LV, EwaldTables E,
-                                                    double *__restrict__ part) {
+                                                    double *__restrict__ part, const float2 *__restrict__ nt,
+                                                    const float2 *__restrict__ sf, float *__restrict__ tpart) {
     __shared__ int4 sy[64];
     const int tid = threadIdx.x;
     const int64_t c = blockIdx.x;
@@ -71,15 +72,16 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
             const int32_t src = lst[e];
             const int32_t sb = pb[src], sn = pe[src] - sb;
             for (int32_t base = 0; base < sn; base += 64) {
-                const int32_t nt = min(64, sn - base);
+                const int32_t nsy = min(64, sn - base);
                 __syncthreads();
-                if (tid < nt) sy[tid] = pos[sb + base + tid];
+                if (tid < nsy) sy[tid] = pos[sb + base + tid];
                 __syncthreads();
-                for (int32_t q = 0; q < nt; q++) {
+                for (int32_t q = 0; q < nsy; q++) {
                     const int4 y = sy[q];
                     T dX[3] = {wrap_sep_t<T>(xi[0], y.x), wrap_sep_t<T>(xi[1], y.y), wrap_sep_t<T>(xi[2], y.z)};
                     T ph, g[3];
-                    pp_ewald_pair<T>(E, dX, ph, g);
+                    if constexpr (SEP) pp_ewald_pair_sep(E, dX, ph, g);
+                    else pp_ewald_pair<T>(E, dX, ph, g);
                     aphi.add(m * ph);
                     for (int d = 0; d < 3; d++) ag[d].add(m * g[d]);
                 }
@@ -96,7 +98,8 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
             for (int d = 0; d < 3; d++) dX[d] = sep<T>(xi[d], s.x[d], true);
 #pragma unroll
             for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-            green_ewald_full<T>(E, dX, D);
+            if constexpr (SEP) green_ewald_sep(E, dX, D);
+            else green_ewald_full<T>(E, dX, D);
             T ph, g[3];
             contract_M2P<T>(ph, g, M, D);
             aphi.add(ph);
@@ -108,23 +111,89 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
         o[0] = aphi.get();
         for (int d = 0; d < 3; d++) o[1 + d] = ag[d].get();
     }
+    if constexpr (SEP) {
+        /* this chunk's share of the leaf's reciprocal sums: thread t takes vector h_t */
+        if (tid < NFOUR_HALF) {
+            float a[EW_SEP_K];
+#pragma unroll
+            for (int q = 0; q < EW_SEP_K; q++) a[q] = 0.0f;
+            if (k < npp) {
+                const int32_t *lst = LV.pool[TG_PP_E] + LV.off[TG_PP_E][leaf];
+                const int32_t e1 = min(lpp, (k + 1) * EW_KPP);
+                const float m = P.m_f;
+                for (int32_t e = k * EW_KPP; e < e1; e++) {
+                    const float2 f = sf[(int64_t)lst[e] * NFOUR_HALF + tid];
+                    a[0] += m * f.x;
+                    a[1] += m * f.y;
+                }
+            } else {
+                const int32_t lpc = LV.len[TG_PC_E][leaf];
+                const int32_t *lst = LV.pool[TG_PC_E] + LV.off[TG_PC_E][leaf];
+                const int32_t e0 = (k - npp) * EW_KPC, e1 = min(lpc, e0 + EW_KPC);
+                SepQ Q;
+                sep_q(__ldg(&E.four[tid]), Q);
+                for (int32_t e = e0; e < e1; e++) {
+                    const int32_t src = lst[e];
+                    const float2 f = nt[(int64_t)src * NFOUR_HALF + tid];
+                    const float *M = ms[src].m;
+                    float m2 = 0.0f, m3 = 0.0f, m3p = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < 6; i++) m2 += Q.q2[i] * M[1 + i];
+#pragma unroll
+                    for (int i = 0; i < 10; i++) {
+                        m3 += Q.q3[i] * M[7 + i];
+                        m3p += Q.q3p[i] * M[7 + i];
+                    }
+                    a[0] += M[0] * f.x;
+                    a[1] += M[0] * f.y;
+                    a[2] += m2 * f.x;
+                    a[3] += m2 * f.y;
+                    a[4] += m3p * f.x;
+                    a[5] += m3p * f.y;
+                    a[6] += m3 * f.x;
+                    a[7] += m3 * f.y;
+                }
+            }
+            float *o = tpart + (c * NFOUR_HALF + tid) * EW_SEP_K;
+#pragma unroll
+            for (int q = 0; q < EW_SEP_K; q++) o[q] = a[q];
+        }
+    }
 }
 
-/* add each leaf's chunk sums, in chunk order, to its FP64 accumulators */
+/* add each leaf's chunk sums, in chunk order, to its FP64 accumulators; with
+ * tpart, also the reciprocal part from the chunks' leaf sums (in chunk order) */
 __global__ void __launch_bounds__(64) k_ewald_reduce(const int32_t *__restrict__ leaves, int32_t nleaves,
                                                      const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
                                                      const int32_t *__restrict__ pe, const double *__restrict__ part,
-                                                     double *__restrict__ acc) {
+                                                     double *__restrict__ acc, const float *__restrict__ tpart,
+                                                     const int4 *__restrict__ pos, EwaldTables E) {
+    __shared__ double sT[NFOUR_HALF * EW_SEP_K];
+    __shared__ double sct[NFOUR_HALF];
     const int32_t li = blockIdx.x;
     const int tid = threadIdx.x;
     if (li >= nleaves) return;
     const int32_t leaf = leaves[li];
     const int32_t b = pb[leaf], cnt = pe[leaf] - b;
-    if (tid >= cnt || off[li + 1] == off[li]) return;
+    if (off[li + 1] == off[li]) return;
+    if (tpart) { /* block-uniform */
+        for (int i = tid; i < NFOUR_HALF * EW_SEP_K; i += 64) {
+            double s = 0.0;
+            for (int64_t c = off[li]; c < off[li + 1]; c++) s += (double)tpart[c * NFOUR_HALF * EW_SEP_K + i];
+            sT[i] = s;
+        }
+        for (int t = tid; t < NFOUR_HALF; t += 64) sct[t] = sep_ct(__ldg(&E.four[t]));
+        __syncthreads();
+    }
+    if (tid >= cnt) return;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t c = off[li]; c < off[li + 1]; c++)
 #pragma unroll
         for (int q = 0; q < 4; q++) v[q] += part[4 * (c * 64 + tid) + q];
+    if (tpart) {
+        const int4 p = pos[b + tid];
+        sep_eval(E, sT, sct, p.x, p.y, p.z, v[0], v + 1);
+    }
     double *o = acc + 4 * (int64_t)(b + tid);
 #pragma unroll
     for (int q = 0; q < 4; q++) o[q] += v[q];

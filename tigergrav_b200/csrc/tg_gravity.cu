@@ -529,6 +529,7 @@ __device__ __forceinline__ int32_t rel_off(int32_t Y, int32_t Xr, bool per, uint
 }
 
 #include "tg_pp.cuh"
+#include "tg_ewald_sep.cuh"
 #include "tg_ewald_leaf.cuh"
 
 /* ---------------- kernel-level seams ---------------- */
@@ -688,14 +689,28 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     TG_CUDA(cudaStreamSynchronize(st));
     if (total <= 0) return TG_OK;
     TG_TRY(ensure(S.ew_part, (size_t)total * 64 * 4));
-    if (f64)
-        k_ewald_chunk<double><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
-                                                    S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p);
-    else
-        k_ewald_chunk<float><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
-                                                   S.pos.p, LV, E, S.ew_part.p);
+    float *tpart = nullptr;
+    if (f64) {
+        k_ewald_chunk<double, false><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
+                                                           S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, nullptr, nullptr,
+                                                           nullptr);
+    } else {
+        /* reciprocal terms per sink leaf: (cos, sin) tables per node, sums per leaf */
+        const int64_t nn = S.nnodes;
+        TG_TRY(ensure(S.ew_nt, (size_t)nn * NFOUR_HALF));
+        TG_TRY(ensure(S.ew_sf, (size_t)nn * NFOUR_HALF));
+        TG_TRY(ensure(S.ew_tpart, (size_t)total * NFOUR_HALF * EW_SEP_K));
+        tpart = S.ew_tpart.p;
+        k_ewald_sf<<<(int)((nn * 32 + 127) / 128), 128, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p,
+                                                                S.pos.p, E, S.ew_nt.p, S.ew_sf.p);
+        TG_TRY(launched(S));
+        k_ewald_chunk<float, true><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
+                                                         S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, S.ew_nt.p, S.ew_sf.p,
+                                                         tpart);
+    }
     TG_TRY(launched(S));
-    k_ewald_reduce<<<nleaves, 64, 0, st>>>(S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.ew_part.p, S.accd.p);
+    k_ewald_reduce<<<nleaves, 64, 0, st>>>(S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.ew_part.p, S.accd.p,
+                                           tpart, S.pos.p, E);
     TG_TRY(launched(S));
     return TG_OK;
 }

@@ -123,6 +123,8 @@ struct Solver {
     DevBuf<double> ew_Hd;
     DevBuf<float4> ew_Pf;
     DevBuf<double2> ew_Pd;
+    DevBuf<float2> ew_nt, ew_sf; /* per node and h: (cos, sin) at the centre of mass; per leaf: sums over particles */
+    DevBuf<float> ew_tpart;      /* per leaf Ewald chunk and h: 8 reciprocal-space source sums */
     bool have_tables = false;
 
     /* rung (individual) time steps: the rung lives in vel[i].w */
