@@ -40,7 +40,7 @@
 namespace tg {
 
 constexpr int FOF_STACK = 128;
-constexpr int FOF_TPB = 256;
+constexpr int FOF_TPB = 64; /* threads per group in the catalogue (most groups have 2-3 members) */
 
 __global__ void k_fof_init(int64_t n, int32_t *P, int64_t *__restrict__ gmin, uint8_t *__restrict__ has_friend) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -223,7 +223,6 @@ __global__ void k_fof_out(int64_t n, const int32_t *__restrict__ R, const int4 *
  * memory.  All sums run in a fixed order: deterministic.
  * stats per group (13 doubles): x[3], v[3], dv[3], rmax, N, id, rc
  */
-static_assert(FOF_TPB == 256, "one histogram bin per thread");
 __global__ void __launch_bounds__(FOF_TPB) k_group_stats(int64_t n, const int32_t *__restrict__ roots,
                                                          const int32_t *__restrict__ off,
                                                          const int32_t *__restrict__ cnt, const int32_t *__restrict__ member,
@@ -307,7 +306,7 @@ __global__ void __launch_bounds__(FOF_TPB) k_group_stats(int64_t n, const int32_
     /* element N/2 of the sorted radii: radix select, 8 bits a pass from the top */
     unsigned int mask = 0u;
     for (int shift = 24; shift >= 0; shift -= 8) {
-        hist[threadIdx.x] = 0u;
+        for (int q = threadIdx.x; q < 256; q += FOF_TPB) hist[q] = 0u;
         __syncthreads();
         const unsigned int pre = sel_prefix;
         for (int32_t j = threadIdx.x; j < N; j += FOF_TPB) {
