@@ -143,20 +143,15 @@ __device__ __forceinline__ void pp_ewald_pair_sep(const EwaldTables &E, const fl
     g[2] = gz + dX0[2] * f0;
 }
 
-/* green_ewald without its reciprocal terms (FP32).  At r <= 1e-6 it is phi0
- * alone; with SUB minus the reciprocal terms the sink's sums include for this
- * source (without SUB the caller leaves the source out of those sums). */
-template <bool SUB = true>
+/* green_ewald without its reciprocal terms (FP32) */
 __device__ __forceinline__ void green_ewald_sep(const EwaldTables &E, const float *X, float *D) {
 #pragma unroll
     for (int k = 0; k < LP; k++) D[k] = 0.0f;
     const float r2 = X[0] * X[0] + X[1] * X[1] + X[2] * X[2];
-    if (!(r2 > 1.0e-12f)) {
-        if constexpr (SUB) {
-            for (int t = 0; t < NFOUR_HALF; t++) ewald_four_term<float>(D, X, __ldg(&E.four[t]), E.Hf + HS * t);
+    if (!(r2 > 1.0e-12f)) { /* phi0 alone, minus the reciprocal terms the leaf sums add */
+        for (int t = 0; t < NFOUR_HALF; t++) ewald_four_term<float>(D, X, __ldg(&E.four[t]), E.Hf + HS * t);
 #pragma unroll
-            for (int k = 0; k < LP; k++) D[k] = -D[k];
-        }
+        for (int k = 0; k < LP; k++) D[k] = -D[k];
         D[E0()] += EWALD_PHI0;
         return;
     }

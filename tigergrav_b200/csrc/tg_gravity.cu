@@ -229,7 +229,7 @@ __device__ __forceinline__ void green_ewald_full(const EwaldTables &E, const T *
  * terms, plus, on lane 0, the final assembly.  The sum of the 32 partial
  * results is green_ewald; the M2L / P2L contractions are linear, so each lane
  * contracts its own part.  X must not be 0 (the caller handles r <= 1e-6). */
-template <class T, bool FOUR = true>
+template <class T>
 __device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *X, T *D, int lane) {
 #pragma unroll
     for (int k = 0; k < LP; k++) D[k] = T(0);
@@ -250,11 +250,10 @@ __device__ __forceinline__ void green_ewald_warp(const EwaldTables &E, const T *
         }
     }
     ewald_mom_finish<T>(D, mom);
-    if constexpr (FOUR)
-        for (int t = lane; t < NFOUR_HALF; t += 32) {
-            const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
-            ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
-        }
+    for (int t = lane; t < NFOUR_HALF; t += 32) {
+        const T *H = (sizeof(T) == 4) ? (const T *)(E.Hf + HS * t) : (const T *)(E.Hd + HS * t);
+        ewald_four_term<T>(D, X, __ldg(&E.four[t]), H);
+    }
     if (lane == 0) {
         if constexpr (sizeof(T) == 4) D[E0()] += T(0.78539816339744831);
         else ewald_finish<T, T>(D, X);
@@ -333,7 +332,6 @@ __global__ void __launch_bounds__(128) k_node(GParams P, int64_t nn, const int32
     }
 }
 
-#include "tg_ewald_sep.cuh"
 #include "tg_ewald_node.cuh"
 
 /* ---- L2L, one level ---- */
@@ -531,6 +529,7 @@ __device__ __forceinline__ int32_t rel_off(int32_t Y, int32_t Xr, bool per, uint
 }
 
 #include "tg_pp.cuh"
+#include "tg_ewald_sep.cuh"
 #include "tg_ewald_leaf.cuh"
 
 /* ---------------- kernel-level seams ---------------- */
@@ -660,19 +659,13 @@ static int node_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     if (total <= 0) return TG_OK;
     TG_TRY(ensure(S.ew_part, (size_t)total * LP));
     const int g = (int)(((int64_t)total * 32 + 127) / 128);
-    if (f64) {
-        k_node_ewald<double, false><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
-                                                       S.pos.p, LV, E, S.ew_part.p, nullptr, nullptr, nullptr);
-        TG_TRY(launched(S));
-    } else {
-        TG_TRY(ensure(S.ew_tpart, (size_t)total * NFOUR_HALF * EN_SEP_K));
-        k_node_ewald<float, true><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p,
-                                                     S.pos.p, LV, E, S.ew_part.p, S.ew_nt.p, S.ew_sf.p, S.ew_tpart.p);
-        TG_TRY(launched(S));
-        k_node_ewald_recip<<<(int)((nn * 32 + 127) / 128), 128, 0, st>>>(nn, S.ew_off.p, S.ew_tpart.p, S.nd_ms.p, E,
-                                                                        S.nd_Lloc.p);
-        TG_TRY(launched(S));
-    }
+    if (f64)
+        k_node_ewald<double><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                                E, S.ew_part.p);
+    else
+        k_node_ewald<float><<<g, 128, 0, st>>>(P, nn, total, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
+                                               E, S.ew_part.p);
+    TG_TRY(launched(S));
     k_node_ewald_reduce<<<(int)((nn * LP + 255) / 256), 256, 0, st>>>(nn, S.ew_off.p, S.ew_part.p, S.nd_Lloc.p);
     TG_TRY(launched(S));
     return TG_OK;
@@ -702,9 +695,15 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
                                                            S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, nullptr, nullptr,
                                                            nullptr);
     } else {
-        /* reciprocal terms per sink leaf from the phase tables of gravity_forces */
+        /* reciprocal terms per sink leaf: (cos, sin) tables per node, sums per leaf */
+        const int64_t nn = S.nnodes;
+        TG_TRY(ensure(S.ew_nt, (size_t)nn * NFOUR_HALF));
+        TG_TRY(ensure(S.ew_sf, (size_t)nn * NFOUR_HALF));
         TG_TRY(ensure(S.ew_tpart, (size_t)total * NFOUR_HALF * EW_SEP_K));
         tpart = S.ew_tpart.p;
+        k_ewald_sf<<<(int)((nn * 32 + 127) / 128), 128, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p,
+                                                                S.pos.p, E, S.ew_nt.p, S.ew_sf.p);
+        TG_TRY(launched(S));
         k_ewald_chunk<float, true><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
                                                          S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, S.ew_nt.p, S.ew_sf.p,
                                                          tpart);
@@ -757,14 +756,6 @@ int gravity_forces(Solver &S, cudaStream_t st) {
     if (!f64) TG_TRY(ensure(S.acc, n));
     S.pp_timed = false;
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[3], st));
-    if (!f64 && S.prm.ewald) {
-        /* phase tables for the reciprocal-space sums of the FP32 Ewald kernels */
-        TG_TRY(ensure(S.ew_nt, (size_t)nn * NFOUR_HALF));
-        TG_TRY(ensure(S.ew_sf, (size_t)nn * NFOUR_HALF));
-        k_ewald_sf<<<(int)((nn * 32 + 127) / 128), 128, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p,
-                                                                S.pos.p, E, S.ew_nt.p, S.ew_sf.p);
-        TG_TRY(launched(S));
-    }
     TG_TRY(node_stage(S, P, LV, E, st));
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[4], st));
     const int32_t nleaves = (int32_t)S.st.leaves;
