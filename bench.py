@@ -68,16 +68,17 @@ PP_FLOPS = 26
 # rsqrt and powers of 1/r 8, erfc/exp 18, d0..d4 31, the moment sums 120 ->
 # 185; 38.8 images on average inside the FP32 cut r < 2.1 (4/3 pi 2.1^3);
 # finish 105 -> 7.3k per green_ewald without its reciprocal terms.  The 61
-# reciprocal terms are not evaluated per interaction: each chunk sums its
-# sources' m_k (cos, sin) per vector h (tg_ewald_sep.cuh), per CC_E source
-# and h: separation test 8, m_2 12, m_3 20, six sums 12 -> 52, x 61 = 3.2k;
-# per PC_E source node the same 56 ops x 61 are shared by the sink leaf's
-# particles (~32: +110 per interaction); per PP_E / CP_E source leaf 4 x 61
-# shared by its pairs (negligible).  The per-sink evaluation of the sums (61
-# terms per particle or node) is not counted.  Contractions: M2L 858, M2P
-# 414, P2L 70 (direct kernels: the reference's constants).
+# reciprocal terms of PC_E / PP_E are not evaluated per interaction: each chunk sums its
+# sources' m_k (cos, sin) per vector h in the leaf kernels (tg_ewald_sep.cuh):
+# per PC_E source node 56 ops x 61 shared by the sink leaf's particles (~32:
+# +110 per interaction); per PP_E source leaf 4 x 61 shared by its pairs
+# (negligible).  The per-particle evaluation of the sums (61 terms) is not
+# counted.  The node kernels keep the per-interaction reciprocal sum: one term
+# of the half sum h.X 5, reduction and sin/cos 5, 35 FMAs 70 -> 80, x 61 =
+# 4.9k.  Contractions: M2L 858, M2P 414, P2L 70 (direct kernels: the
+# reference's constants).
 # PP_E pair (cut r < 2, origin separate): 32.5 images x 44 + 30 = 1.46k.
-NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 11400, "CP_E": 7400}
+NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 13100, "CP_E": 12300}
 LEAF_FLOPS = {"PC_D": 581, "PC_E": 7800, "PP_E": 1460}
 
 
@@ -456,7 +457,7 @@ def bench_batch(args, w, cfg):
 # dram__bytes_write.sum over its interactions); scaled by this run's counts,
 # assuming traffic in proportion to interactions (PC_E / CP_E at the rate of
 # PP_E / CC_E, which that capture does not contain).
-TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 27.4, "CP_E": 27.4}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
+TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.2, "CP_E": 6.2}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
 
 
 def roofline(phase_ms, cnt, peak):
@@ -465,7 +466,7 @@ def roofline(phase_ms, cnt, peak):
     kernel source, FMA = 2) / that kernel's CUDA-event phase time."""
     leaf_far = max(phase_ms["leaves"] - phase_ms.get("pp", 0.0), 1e-9)
     kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
-            "k_node + k_node_ewald<float,true> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
+            "k_node + k_node_ewald<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
             "k_ewald_chunk<float,true> + k_leaf<float,64,false> (PC/PP Ewald chunks, L2P, PC direct)":
                 (leaf_far, LEAF_FLOPS, "leaf")}
     name = max(kern, key=lambda k: kern[k][0])
