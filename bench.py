@@ -457,7 +457,7 @@ def bench_batch(args, w, cfg):
 # dram__bytes_write.sum over its interactions); scaled by this run's counts,
 # assuming traffic in proportion to interactions (PC_E / CP_E at the rate of
 # PP_E / CC_E, which that capture does not contain).
-TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.2, "CP_E": 6.2}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
+TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.3, "CP_E": 6.3}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
 
 
 def roofline(phase_ms, cnt, peak):
