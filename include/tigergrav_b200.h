@@ -224,7 +224,8 @@ int tg_find_groups(tg_solver *s, double link_len, int64_t *group, int64_t *ngrou
  * runs zero it by testing opts.ewald for opts.cosmic).  Forces of inactive
  * particles are not evaluated, so tg_get_forces answers TG_ERR_STATE after a
  * step without all_forces.  Rungs start at 0 (tg_set_particles) and travel
- * with the particles; tg_get_rungs reads them in caller order (n int8). */
+ * with the particles; tg_get_rungs reads them in caller order (n int8).  On an
+ * error *state is left as it was (the particles may have drifted). */
 typedef struct {
     double t_max;  /* options::t_max */
     double dt_max; /* options::dt_max */

@@ -176,20 +176,22 @@ extern "C" int tg_rung_step(tg_solver *s, const tg_rung_params *p, tg_rung_state
     if (state->max_rung > tg::RUNG_MAX) return TG_ERR_ARG;
     TG_CUDA(cudaSetDevice(S.dev));
     cudaStream_t st = (cudaStream_t)stream;
+    uint32_t itime = state->itime; /* the state changes only when the whole step succeeds */
     if (state->max_rung >= 0) {
         /* drift by the step of the largest rung, advance the integer time (src/main.cpp:284-299) */
         TG_TRY(tg::drift(S, tg::rung_dt(p->t_max, state->max_rung), st));
-        state->itime += 1u << (31 - state->max_rung);
+        itime += 1u << (31 - state->max_rung);
     }
-    const int mr = tg::host_min_rung(state->itime);
+    const int mr = tg::host_min_rung(itime);
     int64_t na = 0;
     TG_TRY(tg::solve_active(S, mr, all_forces != 0, &na, st));
     int max_rung = 0;
     TG_TRY(tg::rung_kick(S, *p, mr, &max_rung, st));
+    state->itime = itime;
     state->min_rung = mr;
     state->max_rung = max_rung;
     state->num_active = na;
-    state->t = ((double)state->itime / 2147483648.0) * p->t_max; /* time_to_double */
+    state->t = ((double)itime / 2147483648.0) * p->t_max; /* time_to_double */
     return TG_OK;
 }
 
