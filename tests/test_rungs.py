@@ -121,3 +121,34 @@ def test_rung_step_forces_state():
         # a step far below t_max / 2^30 is refused
         with pytest.raises(_lib.TGError):
             s.rung_step(st, t_max=T_MAX, dt_max=T_MAX * 1e-12, eta=ETA)
+
+
+def test_oracle_stepper_time_line():
+    """The oracle's main loop with a fixed force field: particle k has |g| chosen
+    for rung k + 1, so the steps follow the finest rung and each particle is
+    active exactly when its step divides the integer time."""
+    t_max, h, eta = 1.0, 1e-3, 0.1
+    # dt = eta sqrt(h / 2.8 / a) = 2^-(k+1) exactly at a_k; take a little above it
+    a = np.array([(eta / 2.0 ** -(k + 1)) ** 2 * h / 2.8 * 1.001 for k in range(4)])
+    g = np.zeros((4, 3), np.float32)
+    g[:, 0] = a
+    x0 = np.zeros((4, 3), np.int32)
+
+    def forces(x, v):
+        return g
+
+    def drift(x, v, dt):
+        return x
+
+    st = orung.Stepper(x0, np.zeros((4, 3), np.float32), forces, drift, t_max, 0.5, eta, h)
+    first = st.step()
+    assert first["itime"] == 0 and first["min_rung"] == 0 and first["num_active"] == 4
+    assert st.rung.tolist() == [2, 3, 4, 5] and first["max_rung"] == 5
+    seen = []
+    for _ in range(32):
+        s = st.step()
+        seen.append((s["itime"], s["min_rung"], s["num_active"]))
+        assert s["itime"] % (1 << (31 - 5)) == 0  # steps of the finest rung
+    # particle k (rung k + 2) is active every 2^(5 - (k + 2)) steps
+    counts = [sum(1 for _, m, _ in seen if m <= r) for r in (2, 3, 4, 5)]
+    assert counts == [32 // 8, 32 // 4, 32 // 2, 32]
