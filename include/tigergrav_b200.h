@@ -109,8 +109,16 @@ int tg_get_particles(tg_solver *s, int32_t *x, float *v, int where, void *stream
 int tg_build(tg_solver *s, void *stream);
 /* tree::compute_multipoles (src/tree.cpp:203-296). */
 int tg_multipoles(tg_solver *s, void *stream);
-/* tree::kick_fmm list generation (src/tree.cpp:378-635). */
+/* tree::kick_fmm list generation (src/tree.cpp:378-635).  The list pools are
+ * sized from the tree, then from the totals of the last walk; a walk that
+ * overflows a pool writes nothing out of bounds, regrows the pools to the
+ * totals it asked for and runs again (stats.walk_retries counts the reruns). */
 int tg_walk(tg_solver *s, void *stream);
+/* First capacity (entries) of every list pool and of the walk's scratch for
+ * the following walks, 0 = sized from the tree (the default).  A small value
+ * forces the regrowth path; the lists it ends with are the same.  No
+ * counterpart in the reference (its lists are std::vectors). */
+int tg_set_walk_capacity(tg_solver *s, int64_t entries);
 /* kick_fmm evaluation: CC/CP, L2L, L2P, PC/PP, direct and Ewald. */
 int tg_forces(tg_solver *s, void *stream);
 /* solve_gravity (src/main.cpp:31-73): build + multipoles + walk + forces. */
@@ -136,7 +144,8 @@ int tg_energy(tg_solver *s, double out[5], void *stream);
  * memory; n <= TG_NOALLOC_MAX_N, else TG_ERR_SIZE.  The partial sums live in a
  * fixed 2.5 MiB array inside the library, shared by every call: calls that
  * overlap on the GPU race.  The first call on a device looks the array up
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * (cudaGetSymbolAddress); make it before any stream capture.  The call runs
+ * on `device` and leaves the calling thread's current device as it was. */
 #define TG_NOALLOC_MAX_N (1ll << 26)
 int tg_energy_noalloc(const float *v, const float *phi, int64_t n, double m, double G, double *out,
                       int device, void *stream);
@@ -222,10 +231,13 @@ int tg_find_groups(tg_solver *s, double link_len, int64_t *group, int64_t *ngrou
  * max_rung returns the largest new rung of the active particles.  Non-
  * cosmological; the second half kick is 0.5 dt (the reference's periodic
  * runs zero it by testing opts.ewald for opts.cosmic).  Forces of inactive
- * particles are not evaluated, so tg_get_forces answers TG_ERR_STATE after a
- * step without all_forces.  Rungs start at 0 (tg_set_particles) and travel
- * with the particles; tg_get_rungs reads them in caller order (n int8).  On an
- * error *state is left as it was (the particles may have drifted). */
+ * particles are not evaluated and the lists hold active sinks only, so after
+ * a step without all_forces tg_forces, tg_get_forces, tg_tidal and tg_get_list
+ * answer TG_ERR_STATE until the next full solve.  Rungs start at 0
+ * (tg_set_particles) and travel with the particles; tg_get_rungs reads them in
+ * caller order (n int8).  On an error *state is left as it was, and so are the
+ * velocities and rungs (a rung overflow is found before any kick is applied);
+ * the positions may have drifted. */
 typedef struct {
     double t_max;  /* options::t_max */
     double dt_max; /* options::dt_max */

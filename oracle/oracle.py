@@ -30,9 +30,9 @@ class Params(C.Structure):
 def build(with_ref: bool = True) -> None:
     """Compile the oracle (and, when the reference tree exists, its kernels)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "libtg_oracle.so"])
-    if with_ref and os.path.isdir(os.environ.get("TG_REFERENCE", "/root/reference")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref",
-                               "REF=" + os.environ.get("TG_REFERENCE", "/root/reference")])
+    if with_ref:
+        extra = ["REF=" + os.environ["TG_REFERENCE"]] if os.environ.get("TG_REFERENCE") else []
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref-if-present"] + extra)
 
 
 _lib = None

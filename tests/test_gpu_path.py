@@ -7,7 +7,6 @@ tests/test_oracle_golden.py).
   forces    FP64 path vs the oracle's FP64 evaluation: 1e-6; FP32 path vs the
             reference's arithmetic: 1e-5 per particle (99th percentile)
 """
-import os
 
 import numpy as np
 import pytest
@@ -132,9 +131,6 @@ def test_forces(name, precision, oracle_mod):
         assert np.abs(phi - o64phi).max() / prms < 1e-6
         return
     e = rel_force_err(gg, o32g)
-    if (np.percentile(e, 99) >= FORCE_TOL or e.max() >= 10 * FORCE_TOL) and os.path.isdir("gpurun_out"):
-        np.savez("gpurun_out/fail_%s_%s.npz" % (name, precision), phi=phi, g=gg, o32phi=o32phi, o32g=o32g,
-                 o64phi=o64phi, o64g=o64g, x=g["x"], perm=g["perm"])
     assert np.percentile(e, 99) < FORCE_TOL, np.percentile(e, 99)
     assert e.max() < 10 * FORCE_TOL, (e.max(), np.argmax(e))
     assert np.linalg.norm(gg - o32g, axis=1).max() / rms < 5 * FORCE_TOL

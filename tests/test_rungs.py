@@ -109,18 +109,33 @@ def test_rung_step_forces_state():
     with GravitySolver(len(x), theta=0.7) as s, GravitySolver(len(x), theta=0.7) as full:
         s.set_particles(x)
         st = s.rung_step(None, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
-        st = s.rung_step(st, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
-        if st["num_active"] < len(x):
-            with pytest.raises(_lib.TGError):
-                s.get_forces()
+        for _ in range(8):  # until a step with inactive particles
+            st = s.rung_step(st, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+            if st["num_active"] < len(x):
+                break
+        assert st["num_active"] < len(x)
+        # the lists of a gated step hold active sinks only: no call may serve
+        # forces or lists from them until the next full solve
+        with pytest.raises(_lib.TGError):
+            s.get_forces()
+        with pytest.raises(_lib.TGError):
+            s.forces()
+        with pytest.raises(_lib.TGError):
+            s.tidal(np.zeros((len(x), 3)))
+        with pytest.raises(Exception):
+            s.list("PP_D")
         # with all_forces every particle is a sink: forces equal a full solve's
         st = s.rung_step(st, t_max=T_MAX, dt_max=DT_MAX, eta=ETA, all_forces=True)
         xs, vs = s.get_particles()
         full.set_particles(xs, vs).solve_gravity()
         assert np.array_equal(s.get_forces(dtype=np.float32)[1], full.get_forces(dtype=np.float32)[1])
-        # a step far below t_max / 2^30 is refused
+        # a step far below t_max / 2^30 is refused before any kick: velocities
+        # and rungs stay as they were (only the drift has happened)
+        v_before, r_before = s.get_particles()[1], s.rungs()
         with pytest.raises(_lib.TGError):
             s.rung_step(st, t_max=T_MAX, dt_max=T_MAX * 1e-12, eta=ETA)
+        assert np.array_equal(s.get_particles()[1], v_before)
+        assert np.array_equal(s.rungs(), r_before)
 
 
 def test_oracle_stepper_time_line():

@@ -49,7 +49,7 @@ class tg_stats(C.Structure):
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
     "tg_error_string", "tg_version", "tg_create", "tg_destroy", "tg_set_particles", "tg_get_particles",
-    "tg_build", "tg_multipoles", "tg_walk", "tg_forces", "tg_solve_gravity", "tg_get_forces",
+    "tg_build", "tg_multipoles", "tg_walk", "tg_set_walk_capacity", "tg_forces", "tg_solve_gravity", "tg_get_forces",
     "tg_get_forces_f64", "tg_kick", "tg_drift", "tg_energy", "tg_leapfrog", "tg_get_stats", "tg_num_nodes",
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
@@ -84,6 +84,7 @@ def _load():
     L.tg_get_particles.argtypes = [vp, vp, vp, i32, vp]
     for f in ("tg_build", "tg_multipoles", "tg_walk", "tg_forces", "tg_solve_gravity"):
         getattr(L, f).argtypes = [vp, vp]
+    L.tg_set_walk_capacity.argtypes = [vp, i64]
     L.tg_get_forces.argtypes = [vp, vp, vp, i32, vp]
     L.tg_get_forces_f64.argtypes = [vp, vp, vp, i32, vp]
     L.tg_kick.argtypes = [vp, d, vp]

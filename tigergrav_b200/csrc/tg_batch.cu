@@ -155,18 +155,21 @@ int tg_batch_autotune(tg_batch *b, const int32_t *leaf_sizes, int32_t nsizes, in
             tg::Solver &S = b->box[i]->S;
             S.prm.leaf_max = leaf_sizes[k];
             TG_TRY(tg_solve_gravity(b->box[i], st)); /* warm-up: buffers sized for this leaf size */
-            cudaEvent_t e0, e1;
-            TG_CUDA(cudaEventCreate(&e0));
-            TG_CUDA(cudaEventCreate(&e1));
-            TG_CUDA(cudaEventRecord(e0, st));
-            const int r = tg_solve_gravity(b->box[i], st);
-            TG_CUDA(cudaEventRecord(e1, st));
-            TG_CUDA(cudaEventSynchronize(e1));
+            struct Events { /* destroyed on every return path */
+                cudaEvent_t e[2] = {nullptr, nullptr};
+                ~Events() {
+                    for (cudaEvent_t x : e)
+                        if (x) cudaEventDestroy(x);
+                }
+            } ev;
+            TG_CUDA(cudaEventCreate(&ev.e[0]));
+            TG_CUDA(cudaEventCreate(&ev.e[1]));
+            TG_CUDA(cudaEventRecord(ev.e[0], st));
+            TG_TRY(tg_solve_gravity(b->box[i], st));
+            TG_CUDA(cudaEventRecord(ev.e[1], st));
+            TG_CUDA(cudaEventSynchronize(ev.e[1]));
             float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            if (r != TG_OK) return r;
+            TG_CUDA(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1])); /* a failed timing is an error, not 0 ms */
             if (ms < best[i]) {
                 best[i] = ms;
                 pick[i] = leaf_sizes[k];

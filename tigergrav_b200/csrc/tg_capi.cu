@@ -404,6 +404,17 @@ int tg_walk(tg_solver *s, void *stream) {
     return tree_walk(s->S, STREAM(stream));
 }
 
+int tg_set_walk_capacity(tg_solver *s, int64_t entries) {
+    CHECK_HANDLE(s);
+    if (entries < 0) return TG_ERR_ARG;
+    tg::Solver &S = s->S;
+    S.cap_start = entries;
+    for (int k = 0; k < tg::NLIST; k++) S.list_cap[k] = 0;
+    S.nx_cap = 0;
+    if (entries > 0) S.scratch_per_warp = 0;
+    return TG_OK;
+}
+
 int tg_forces(tg_solver *s, void *stream) {
     CHECK_HANDLE(s);
     return gravity_forces(s->S, STREAM(stream));

@@ -101,6 +101,19 @@ __global__ void k_energy_noalloc_final(int64_t nparts, const double *__restrict_
     }
 }
 
+/* the launches of one call, with `device` current */
+static int energy_noalloc_on(const float *v, const float *phi, int64_t n, double m, double G, double *out,
+                             int device, cudaStream_t st) {
+    double *part = nullptr;
+    TG_TRY(noalloc_scratch(device, &part));
+    const int64_t nparts = (n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
+    k_energy_noalloc_partial<<<(unsigned)nparts, 256, 0, st>>>(n, v, phi, m, G, part);
+    TG_CUDA(cudaGetLastError());
+    k_energy_noalloc_final<<<1, 256, 0, st>>>(nparts, part, n, out);
+    TG_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 } // namespace tg
 
 extern "C" int tg_energy_noalloc(const float *v, const float *phi, int64_t n, double m, double G, double *out,
@@ -108,14 +121,17 @@ extern "C" int tg_energy_noalloc(const float *v, const float *phi, int64_t n, do
     using namespace tg;
     if (!v || !out || n < 1 || !std::isfinite(m) || !std::isfinite(G)) return TG_ERR_ARG;
     if (n > TG_NOALLOC_MAX_N) return TG_ERR_SIZE;
-    TG_CUDA(cudaSetDevice(device));
-    double *part = nullptr;
-    TG_TRY(noalloc_scratch(device, &part));
-    const int64_t nparts = (n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
-    cudaStream_t st = (cudaStream_t)stream;
-    k_energy_noalloc_partial<<<(unsigned)nparts, 256, 0, st>>>(n, v, phi, m, G, part);
-    TG_CUDA(cudaGetLastError());
-    k_energy_noalloc_final<<<1, 256, 0, st>>>(nparts, part, n, out);
-    TG_CUDA(cudaGetLastError());
-    return TG_OK;
+    /* the caller's thread keeps its current device: switch only for the call */
+    int prev = -1;
+    TG_CUDA(cudaGetDevice(&prev));
+    if (prev != device) TG_CUDA(cudaSetDevice(device));
+    const int rc = energy_noalloc_on(v, phi, n, m, G, out, device, (cudaStream_t)stream);
+    if (prev != device) {
+        const cudaError_t e = cudaSetDevice(prev);
+        if (e != cudaSuccess && rc == TG_OK) {
+            set_last_cuda_error(e, "cudaSetDevice (restoring the caller's device)", __FILE__, __LINE__);
+            return TG_ERR_CUDA;
+        }
+    }
+    return rc;
 }

@@ -59,7 +59,10 @@ __global__ void k_node_active(int64_t nn, const int32_t *__restrict__ pb, const 
     nact[i] = scan[pe[i]] - scan[pb[i]];
 }
 
-/* part_vect_kick for one active particle (src/part_vect.cpp:358-381) */
+/* part_vect_kick for one active particle (src/part_vect.cpp:358-381).
+ * WRITE = false only checks that every new rung is representable (err bit 8),
+ * so a step that fails leaves velocities and rungs untouched. */
+template <bool WRITE>
 __global__ void k_rung_kick(int64_t n, float4 *__restrict__ vel, const float4 *__restrict__ acc,
                             const double *__restrict__ accd, int min_rung, double t_max, double dt_max, double eta,
                             double h, double G, int *__restrict__ max_rung, uint32_t *__restrict__ err) {
@@ -99,6 +102,7 @@ __global__ void k_rung_kick(int64_t n, float4 *__restrict__ vel, const float4 *_
             break;
         }
     }
+    if (!WRITE) return;
     rung = max(rung, min_rung);
     atomicMax(max_rung, rung);
     const float s2 = __double2float_rn(__dmul_rn(__dmul_rn(0.5, rung_dt(t_max, rung)), G));
@@ -142,7 +146,13 @@ static int solve_active(Solver &S, int min_rung, bool all, int64_t *num_active, 
     S.walk_nact = nullptr;
     TG_TRY(rc);
     TG_TRY(gravity_forces(S, st));
-    if (!all) S.have_forces = false; /* forces of inactive leaves were not evaluated */
+    if (!all) {
+        /* forces of inactive leaves were not evaluated, and the lists hold
+         * active sinks only: neither may serve tg_forces, tg_get_forces,
+         * tg_tidal or tg_get_list */
+        S.have_forces = false;
+        S.have_lists = false;
+    }
     return TG_OK;
 }
 
@@ -151,13 +161,19 @@ static int rung_kick(Solver &S, const tg_rung_params &p, int min_rung, int *max_
     const bool f64 = S.prm.precision == TG_PREC_F64;
     TG_CUDA(cudaMemsetAsync(S.dev_cnt.p, 0, sizeof(unsigned long long), st));
     TG_CUDA(cudaMemsetAsync(S.dev_err.p, 0, sizeof(uint32_t), st));
-    k_rung_kick<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.vel.p, f64 ? nullptr : S.acc.p, f64 ? S.accd.p : nullptr,
-                                                        min_rung, p.t_max, p.dt_max, p.eta, S.prm.soft_len, S.prm.G,
-                                                        (int *)S.dev_cnt.p, S.dev_err.p);
+    const int nb = (int)((n + 255) / 256);
+    /* check pass first: on a rung overflow nothing is kicked */
+    k_rung_kick<false><<<nb, 256, 0, st>>>(n, S.vel.p, f64 ? nullptr : S.acc.p, f64 ? S.accd.p : nullptr, min_rung,
+                                           p.t_max, p.dt_max, p.eta, S.prm.soft_len, S.prm.G, (int *)S.dev_cnt.p,
+                                           S.dev_err.p);
     TG_TRY(launched(S));
     uint32_t err = 0;
     TG_TRY(read_err(S, st, &err));
     if (err) return TG_ERR_ARG; /* a step below t_max / 2^30 */
+    k_rung_kick<true><<<nb, 256, 0, st>>>(n, S.vel.p, f64 ? nullptr : S.acc.p, f64 ? S.accd.p : nullptr, min_rung,
+                                          p.t_max, p.dt_max, p.eta, S.prm.soft_len, S.prm.G, (int *)S.dev_cnt.p,
+                                          S.dev_err.p);
+    TG_TRY(launched(S));
     int mr = 0;
     TG_CUDA(cudaMemcpyAsync(&mr, S.dev_cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));

@@ -99,7 +99,9 @@ struct Solver {
     DevBuf<int32_t> scratch;             /* leaf drain per-warp scratch */
     int64_t scratch_per_warp = 0;
     int drain_warps = 0;
-    int walk_retries = 0;
+    int64_t list_cap[NLIST] = {0, 0, 0, 0, 0, 0, 0, 0}; /* pool capacities that served the last walk */
+    int64_t nx_cap = 0;
+    int64_t cap_start = 0; /* tg_set_walk_capacity: first capacity of every pool (0: sized from the tree) */
 
     /* status / stats */
     DevBuf<uint32_t> dev_err;

@@ -28,6 +28,8 @@
  * and iterates in a private global scratch area.  Capacity overflows never
  * write out of bounds: they set a flag and the host regrows and repeats.
  */
+#include <algorithm>
+
 #include "tg_solver.cuh"
 
 namespace tg {
@@ -441,24 +443,26 @@ int tree_walk(Solver &S, cudaStream_t st) {
     TG_CUDA(cudaStreamSynchronize(st));
     const int32_t nleaves = (int32_t)nleaves_h;
 
-    /* initial capacities (grown on overflow) */
+    /* capacities: those that served the last walk, else sized from the tree;
+     * on an overflow the pools grow to the totals the walk asked for */
     int64_t cap[NLIST];
     int64_t cap_nx = 0;
     {
         const int64_t base_nodes = nn + 64;
         const int64_t base_leaves = nleaves + 64;
-        int64_t mult = 1;
-        for (int q = 0; q < S.walk_retries; q++) mult *= 2;
-        cap[TG_CC_D] = 160 * base_nodes * mult;
-        cap[TG_CP_D] = 16 * base_nodes * mult;
-        cap[TG_CC_E] = (S.prm.ewald ? 32 : 1) * base_nodes * mult;
-        cap[TG_CP_E] = (S.prm.ewald ? 8 : 1) * base_nodes * mult;
-        cap[TG_PC_D] = 16 * base_leaves * mult;
-        cap[TG_PP_D] = 96 * base_leaves * mult;
-        cap[TG_PC_E] = (S.prm.ewald ? 16 : 1) * base_leaves * mult;
-        cap[TG_PP_E] = (S.prm.ewald ? 32 : 1) * base_leaves * mult;
-        cap_nx = 400 * base_nodes * mult;
+        const int64_t dflt[NLIST] = {160 * base_nodes,
+                                     16 * base_nodes,
+                                     (S.prm.ewald ? 32 : 1) * base_nodes,
+                                     (S.prm.ewald ? 8 : 1) * base_nodes,
+                                     16 * base_leaves,
+                                     96 * base_leaves,
+                                     (S.prm.ewald ? 16 : 1) * base_leaves,
+                                     (S.prm.ewald ? 32 : 1) * base_leaves};
+        for (int k = 0; k < NLIST; k++)
+            cap[k] = S.cap_start > 0 ? S.cap_start : (S.list_cap[k] > 0 ? S.list_cap[k] : dflt[k]);
+        cap_nx = S.cap_start > 0 ? S.cap_start : (S.nx_cap > 0 ? S.nx_cap : 400 * base_nodes);
         if (S.scratch_per_warp == 0) S.scratch_per_warp = 4096;
+        if (S.cap_start > 0) S.scratch_per_warp = std::min<int64_t>(S.scratch_per_warp, S.cap_start);
     }
     int tries = 0;
     for (;;) {
@@ -516,19 +520,32 @@ int tree_walk(Solver &S, cudaStream_t st) {
             return TG_ERR_STATE;
         }
         if (!err) break;
-        if (++tries > 8) {
+        if (++tries > 24) {
             release(d_pools);
             release(d_llen);
             release(d_loff);
             release(d_caps);
             return TG_ERR_CAPACITY;
         }
-        if (err & DEV_ERR_OVERFLOW_LIST)
-            for (int k = 0; k < NLIST; k++) cap[k] *= 2;
-        if (err & DEV_ERR_OVERFLOW_NEXT) cap_nx *= 2;
+        /* the pool tops kept counting past a full pool: they are what this
+         * walk asked for (a lower bound when a next-list or scratch overflow
+         * starved the levels below, hence at least doubling then) */
+        unsigned long long tops[NLIST + 2];
+        TG_CUDA(cudaMemcpyAsync(tops, S.pool_top.p, sizeof(tops), cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+        const bool starved = (err & (DEV_ERR_OVERFLOW_NEXT | DEV_ERR_OVERFLOW_SCRATCH)) != 0;
+        for (int k = 0; k < NLIST; k++) {
+            const int64_t want = (int64_t)tops[k] + (int64_t)(tops[k] / 8) + 1024;
+            if ((int64_t)tops[k] > cap[k]) cap[k] = std::max(want, starved ? 2 * cap[k] : want);
+        }
+        if (err & DEV_ERR_OVERFLOW_NEXT) {
+            const int64_t t = (int64_t)std::max(tops[NLIST], tops[NLIST + 1]);
+            cap_nx = std::max(2 * cap_nx, t + t / 8 + 1024);
+        }
         if (err & DEV_ERR_OVERFLOW_SCRATCH) S.scratch_per_warp *= 2;
-        S.walk_retries++;
     }
+    for (int k = 0; k < NLIST; k++) S.list_cap[k] = cap[k];
+    S.nx_cap = cap_nx;
     S.st.walk_retries = tries;
     S.st.leaves = nleaves;
     release(d_pools);

@@ -125,6 +125,12 @@ class GravitySolver:
         check("tg_walk", lib.tg_walk(self.h, _stream(stream)))
         return self
 
+    def set_walk_capacity(self, entries: int):
+        """First capacity of every list pool for the following walks (0: sized
+        from the tree); a small value exercises the regrowth path."""
+        check("tg_set_walk_capacity", lib.tg_set_walk_capacity(self.h, int(entries)))
+        return self
+
     def forces(self, stream=None):
         check("tg_forces", lib.tg_forces(self.h, _stream(stream)))
         return self
