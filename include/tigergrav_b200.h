@@ -100,7 +100,8 @@ int tg_create(const tg_params *params, tg_solver **out);
 int tg_destroy(tg_solver *s);
 
 /* Replaces part_vect_init (src/part_vect.cpp:654-673): loads n particles.
- * x: n*3 int32, v: n*3 float (NULL = zero velocities). */
+ * x: n*3 int32, v: n*3 float (NULL = zero velocities).  n < 1 or a non-finite
+ * velocity gives TG_ERR_ARG (then no particles are loaded). */
 int tg_set_particles(tg_solver *s, const int32_t *x, const float *v, int64_t n, int where, void *stream);
 /* Positions / velocities in the caller's original particle order. */
 int tg_get_particles(tg_solver *s, int32_t *x, float *v, int where, void *stream);
@@ -216,6 +217,11 @@ int tg_load_gadget1(const char *path, double *header, int32_t *x, float *v, int6
  * element N/2 of the sorted radii a |x - centre|), 0.  a: scale factor.  With
  * out == NULL only *ngroups is set; capacity < ngroups gives TG_ERR_SIZE. */
 int tg_find_groups(tg_solver *s, double link_len, int64_t *group, int64_t *ngroups, int where, void *stream);
+/* Hook attempts per union in tg_find_groups' lock-free union-find (default
+ * 65536; 0 and up).  A union that runs out of attempts makes tg_find_groups
+ * answer TG_ERR_TIMEOUT instead of spinning; a small limit injects that fault
+ * from the host.  No counterpart in the reference (serial label propagation). */
+int tg_set_fof_retry_limit(tg_solver *s, int32_t tries);
 
 /* ---- hierarchical (rung) time steps ------------------------------------------
  * tigergrav/time.hpp:12-48, the main loop step (src/main.cpp:266-313) and the

@@ -57,7 +57,7 @@ EXPORTS = [
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
     "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo", "tg_load_gadget1",
-    "tg_find_groups", "tg_group_catalog", "tg_rung_step", "tg_get_rungs",
+    "tg_find_groups", "tg_set_fof_retry_limit", "tg_group_catalog", "tg_rung_step", "tg_get_rungs",
 ]
 
 
@@ -126,6 +126,7 @@ def _load():
     L.tg_leapfrog_cosmo.argtypes = [vp, P(tg_cosmo_params), vp, d, i32, vp]
     L.tg_load_gadget1.argtypes = [C.c_char_p, vp, vp, vp, i64, P(i64)]
     L.tg_find_groups.argtypes = [vp, d, vp, P(i64), i32, vp]
+    L.tg_set_fof_retry_limit.argtypes = [vp, i32]
     L.tg_group_catalog.argtypes = [vp, d, vp, i64, P(i64), vp]
     L.tg_rung_step.argtypes = [vp, P(tg_rung_params), P(tg_rung_state), i32, vp]
     L.tg_get_rungs.argtypes = [vp, vp, i32, vp]

@@ -52,7 +52,9 @@ static int ensure_constants(int dev) {
 
 static int validate(const tg_params *p) {
     if (!p) return TG_ERR_ARG;
-    if (!(p->theta > 0.0) || !(p->soft_len > 0.0) || !(p->m > 0.0) || !std::isfinite(p->G)) return TG_ERR_ARG;
+    if (!(p->theta > 0.0) || !(p->soft_len > 0.0) || !(p->m > 0.0)) return TG_ERR_ARG;
+    if (!std::isfinite(p->theta) || !std::isfinite(p->soft_len) || !std::isfinite(p->m) || !std::isfinite(p->G))
+        return TG_ERR_ARG;
     if (p->leaf_max < 1 || p->leaf_max > 128) return TG_ERR_ARG;
     if (p->precision != TG_PREC_F32 && p->precision != TG_PREC_F64) return TG_ERR_ARG;
     int nd = 0;
@@ -64,11 +66,17 @@ static int validate(const tg_params *p) {
     return TG_OK;
 }
 
-__global__ void k_pack(int64_t n, const int32_t *x, const float *v, int4 *pos, float4 *vel) {
+__global__ void k_pack(int64_t n, const int32_t *x, const float *v, int4 *pos, float4 *vel, uint32_t *err) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     pos[i] = make_int4(x[3 * i], x[3 * i + 1], x[3 * i + 2], (int)i);
-    vel[i] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (v) {
+        q = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0f);
+        /* a NaN / inf velocity would drift into an undefined fixed-point position */
+        if (!isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z)) atomicOr(err, DEV_ERR_NONFINITE);
+    }
+    vel[i] = q;
 }
 
 __global__ void k_unpack(int64_t n, const int4 *pos, const float4 *vel, int32_t *x, float *v) {
@@ -349,10 +357,19 @@ int tg_set_particles(tg_solver *s, const int32_t *x, const float *v, int64_t n, 
             dv = (const float *)S.vel_alt.p;
         }
     }
-    k_pack<<<(int)((n + 255) / 256), 256, 0, st>>>(n, dx, dv, S.pos.p, S.vel.p);
+    if (dv) TG_CUDA(cudaMemsetAsync(S.dev_err.p, 0, sizeof(uint32_t), st));
+    k_pack<<<(int)((n + 255) / 256), 256, 0, st>>>(n, dx, dv, S.pos.p, S.vel.p, S.dev_err.p);
     TG_TRY(launched(S));
-    S.n = n;
     S.have_tree = S.have_multipoles = S.have_lists = S.have_forces = false;
+    if (dv) {
+        uint32_t err = 0;
+        TG_TRY(read_err(S, st, &err));
+        if (err & DEV_ERR_NONFINITE) {
+            S.n = 0; /* nothing loaded: later calls answer TG_ERR_STATE */
+            return TG_ERR_ARG;
+        }
+    }
+    S.n = n;
     S.st.n = n;
     return TG_OK;
 }
@@ -531,7 +548,7 @@ static int at_checkpoint(tg_solver *s, int k, cudaStream_t st) {
     Solver &S = s->S;
     const int64_t n = S.n;
     k_pack<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.ck_x.p + (size_t)3 * n * k, S.ck_v.p + (size_t)3 * n * k,
-                                                   S.pos.p, S.vel.p);
+                                                   S.pos.p, S.vel.p, S.dev_err.p); /* checkpoints are finite */
     TG_TRY(launched(S));
     S.have_tree = S.have_multipoles = S.have_lists = S.have_forces = false;
     TG_TRY(tg_build(s, st));

@@ -753,6 +753,7 @@ enum : uint32_t {
     DEV_ERR_DEPTH = 8u,
     DEV_ERR_BADINDEX = 16u,
     DEV_ERR_SPIN = 32u,
+    DEV_ERR_NONFINITE = 64u, /* a non-finite input value (velocity) */
 };
 
 } // namespace tg

@@ -126,8 +126,8 @@ __device__ __forceinline__ int32_t fof_find(int32_t *P, int32_t x) {
     return x;
 }
 
-__device__ void fof_union(int32_t *P, int32_t a, int32_t b, uint32_t *err) {
-    for (int it = 0; it < 65536; it++) {
+__device__ void fof_union(int32_t *P, int32_t a, int32_t b, int32_t max_tries, uint32_t *err) {
+    for (int it = 0; it < max_tries; it++) {
         a = fof_find(P, a);
         b = fof_find(P, b);
         if (a == b) return;
@@ -159,7 +159,8 @@ __device__ __forceinline__ unsigned long long fof_d2(int4 p, int4 q, int periodi
 /* one warp per candidate leaf pair: join every pair of friends */
 __global__ void k_fof_link(int64_t npairs, const int2 *__restrict__ pairs, const int32_t *__restrict__ pb,
                            const int32_t *__restrict__ pe, const int4 *__restrict__ pos, unsigned long long L2,
-                           int periodic, int32_t *P, uint8_t *__restrict__ has_friend, uint32_t *__restrict__ err) {
+                           int periodic, int32_t *P, uint8_t *__restrict__ has_friend, int32_t max_tries,
+                           uint32_t *__restrict__ err) {
     const int lane = threadIdx.x & 31;
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= npairs) return;
@@ -174,7 +175,7 @@ __global__ void k_fof_link(int64_t npairs, const int2 *__restrict__ pairs, const
             if (d2 < L2 && d2 != 0ull) {
                 fi = true;
                 has_friend[j] = 1;
-                fof_union(P, i, j, err);
+                fof_union(P, i, j, max_tries, err);
             }
         }
         if (fi) has_friend[i] = 1;
@@ -390,7 +391,7 @@ static int fof_run(Solver &S, double link_len, int64_t *group_dev, int64_t *ngro
         const int64_t threads = (int64_t)npairs * 32;
         k_fof_link<<<(int)((threads + 255) / 256), 256, 0, st>>>((int64_t)npairs, S.fof_pairs.p, S.nd_pb.p, S.nd_pe.p,
                                                                  S.pos.p, L2, periodic, S.fof_P.p, S.fof_has.p,
-                                                                 S.dev_err.p);
+                                                                 S.fof_tries, S.dev_err.p);
         TG_TRY(launched(S));
     }
     TG_TRY(ensure(S.fof_key, 2 * n));
@@ -404,6 +405,7 @@ static int fof_run(Solver &S, double link_len, int64_t *group_dev, int64_t *ngro
     TG_TRY(launched(S));
     uint32_t err = 0;
     TG_TRY(read_err(S, st, &err));
+    if (err & 4u) return TG_ERR_TIMEOUT; /* a union ran out of hook attempts */
     if (err) return TG_ERR_CAPACITY;
     TG_CUDA(cudaMemcpyAsync(S.h_cnt, S.dev_cnt.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
@@ -506,5 +508,11 @@ extern "C" int tg_group_catalog(tg_solver *s, double a, double *out, int64_t cap
     std::vector<double> h;
     TG_TRY(tg::fof_catalog(S, a, h, (cudaStream_t)stream));
     if (!h.empty()) std::memcpy(out, h.data(), sizeof(double) * h.size());
+    return TG_OK;
+}
+
+extern "C" int tg_set_fof_retry_limit(tg_solver *s, int32_t tries) {
+    if (!s || tries < 0) return TG_ERR_ARG;
+    s->S.fof_tries = tries;
     return TG_OK;
 }

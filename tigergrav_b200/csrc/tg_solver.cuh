@@ -143,6 +143,7 @@ struct Solver {
     DevBuf<double> fof_stats;
     int64_t fof_ngroups = 0, fof_npairs = 0;
     double fof_link = 0.0; /* linking length of the groups held, 0: none for this tree */
+    int32_t fof_tries = 65536; /* hook attempts per union before the union-find gives up */
 
     /* events for phase timing */
     cudaEvent_t ev[8];
