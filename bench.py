@@ -1,36 +1,52 @@
 """Benchmark: periodic tree gravity on B200 (one JSON line on stdout).
 
 Metric: Mparticles/s per force evaluation at RMS relative force error <= 1e-4
-against the FP64 direct Ewald sum.
+against the FP64 direct Ewald sum; adjoint / forward cost.
 
-Workload (default): 128^3 = 2,097,152 particles on a lattice displaced by a
-seeded Gaussian random field with P(k) ~ k^-2 (rms displacement 0.5 spacing),
-periodic unit box, Ewald on, leaf 64, FP32 path.  The method's error depends
-only on theta; on this workload RMS <= 1e-4 needs theta = 0.2 (measured:
-theta 0.22 -> 1.24e-4, 0.2 -> 8.4e-5; 0.7 -> 7.5e-2), so the headline runs
-at theta = 0.2 and every run re-measures and reports the error.  The same
-workload at the literal theta = 0.7 is measured as well and reported under
-"config_theta_0.7".
+Headline workload (default, ``clustered256``): 256^3 = 16,777,216 particles on a
+lattice displaced by a seeded Gaussian random field with P(k) ~ k^-2 (rms
+displacement 0.5 spacing, seed 8), periodic unit box, Ewald on, leaf 64, the
+FP32 compensated path.  The method's error depends on theta only; on this
+workload RMS <= 1e-4 needs theta = 0.19 (0.2 gives 1.24e-4), so the headline
+runs there and every run re-measures the error at 4096 seeded samples.
 
 A step is one kick-drift-kick leapfrog step at dt = 1e-3: half kick, drift, a
-full force evaluation (tree build, multipoles, walk, all interaction
-kernels), half kick.  value = particles / step time.  Inputs stay resident in
-HBM; L2 is flushed (256 MB write, untimed) between timed steps.  e2e: the
-same evaluation through the public API from page-locked host buffers
-(positions + velocities in, phi + g out, copies inside the timed region).
+full force evaluation (tree build, multipoles, walk, every interaction
+kernel), half kick.  value = particles / step time.  Inputs stay resident in
+HBM; L2 is flushed (256 MB write, untimed) between timed steps.
+
+The same JSON line carries:
+  e2e              the evaluation through the public API from page-locked host
+                   buffers (positions + velocities in, phi + g out, copies
+                   inside the timed region);
+  fp64_path        the plain FP64 path (TG_PREC_F64) on the same particles and
+                   GPU, one force evaluation timed after a warm-up one, with its
+                   error; fp32_over_fp64 = its time / the FP32 evaluation time;
+  adjoint          the differentiation workload: 64^3 clustered (seed 5),
+                   L = sum w.x(T) (w ~ N(0,1), seed 6) after 8 steps at
+                   dt = 1e-3: tg_forward and tg_backward times, their ratio, and
+                   central finite differences (h = 1e-4, FP64 path) on 32
+                   coordinates (seed 7);
+  secondary        the 128^3 clustered box (seed 2) at theta 0.2 and at the
+                   literal theta 0.7;
+  roofline         the dominant interaction kernel against the measured FP32
+                   FMA peak of the GPU;
+  cpu_baseline     the reference's own kernels (src/gravity.cpp compiled from
+                   the reference sources into oracle/_ref) on all host cores.
+
+CPU baseline and --impl reference: a force evaluation of the reference's CPU
+path at 256^3 and theta 0.19 takes hours, so its time is assembled from
+measured parts: the tree build and multipoles (the oracle's serial
+restatement of src/tree.cpp, timed), the walk (restated kick_fmm on all host
+threads, timed in full), and per interaction kind the evaluation's count
+times that kind's host throughput, sampled by running the reference kernel
+over random sinks of this workload with their real lists.  The reference arm
+also times full evaluations with the reference kernels on all host cores
+where one fits in seconds: the 32^3 uniform box and the 128^3 clustered box,
+both at theta 0.7 (``measured_full``).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
   torchrun --nproc-per-node N bench.py --gpus N ...   (independent replicas)
-
-CPU baseline and --impl reference: the reference's own kernels
-(src/gravity.cpp compiled from the reference sources into oracle/_ref) on all
-host cores.  A full evaluation at theta = 0.2 costs thousands of core-seconds,
-so the time is assembled from measured parts: the oracle's tree build,
-multipoles and walk (serial restatement of src/tree.cpp, timed, divided by the
-thread count as if perfectly parallel) plus, per interaction kind, the
-interaction count of this evaluation times that kind's host throughput,
-sampled by running the reference kernel of that kind over random sinks of
-this same workload.
 """
 import argparse
 import json
@@ -46,15 +62,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "clustered256": dict(kind="clustered", nside=256, seed=8, theta_rms=0.19,
+                         label="256^3 clustered P(k)~k^-2, rms displacement 0.5 spacing, seed 8"),
     "clustered128": dict(kind="clustered", nside=128, seed=2, theta_rms=0.2,
-                         label="128^3 clustered P(k)~k^-2, rms displacement 0.5 spacing"),
-    "clustered64": dict(kind="clustered", nside=64, seed=5, theta_rms=0.2, label="64^3 clustered"),
-    "clustered256": dict(kind="clustered", nside=256, seed=8, theta_rms=0.2, label="256^3 clustered"),
-    "uniform32": dict(kind="uniform", n=32768, seed=1, theta_rms=0.3, label="32^3 uniform"),
+                         label="128^3 clustered P(k)~k^-2, rms displacement 0.5 spacing, seed 2"),
+    "clustered64": dict(kind="clustered", nside=64, seed=5, theta_rms=0.2, label="64^3 clustered, seed 5"),
+    "uniform32": dict(kind="uniform", n=32768, seed=1, theta_rms=0.3, label="32^3 uniform, seed 1"),
     "batch64": dict(kind="batch", nboxes=64, seed=4, theta_rms=0.7,
                     label="64 boxes, N = 2^U[12,18], half uniform, half clustered"),
 }
-METRIC = "Mparticles/s per force eval at RMS err<=1e-4 vs FP64 Ewald (128^3 clustered)"
+METRIC = "Mparticles/s per force eval at RMS err<=1e-4 vs FP64 Ewald; adjoint/fwd cost"
 KINDS = ("PP_D", "PP_E", "PC_D", "PC_E", "CC_D", "CC_E", "CP_D", "CP_E")
 
 # FP32 operations per PP pair in k_pp_f32's inner loop, counted from the
@@ -68,18 +85,33 @@ PP_FLOPS = 26
 # rsqrt and powers of 1/r 8, erfc/exp 18, d0..d4 31, the moment sums 120 ->
 # 185; 38.8 images on average inside the FP32 cut r < 2.1 (4/3 pi 2.1^3);
 # finish 105 -> 7.3k per green_ewald without its reciprocal terms.  The 61
-# reciprocal terms of PC_E / PP_E are not evaluated per interaction: each chunk sums its
-# sources' m_k (cos, sin) per vector h in the leaf kernels (tg_ewald_sep.cuh):
-# per PC_E source node 56 ops x 61 shared by the sink leaf's particles (~32:
-# +110 per interaction); per PP_E source leaf 4 x 61 shared by its pairs
-# (negligible).  The per-particle evaluation of the sums (61 terms) is not
-# counted.  The node kernels keep the per-interaction reciprocal sum: one term
-# of the half sum h.X 5, reduction and sin/cos 5, 35 FMAs 70 -> 80, x 61 =
-# 4.9k.  Contractions: M2L 858, M2P 414, P2L 70 (direct kernels: the
-# reference's constants).
+# reciprocal terms of PC_E / PP_E are not evaluated per interaction: each
+# chunk sums its sources' m_k (cos, sin) per vector h in the leaf kernels
+# (tg_ewald_sep.cuh): per PC_E source node 56 ops x 61 shared by the sink
+# leaf's particles (~32: +110 per interaction); per PP_E source leaf 4 x 61
+# shared by its pairs (negligible).  The per-particle evaluation of the sums
+# (61 terms) is not counted.  The node kernels keep the per-interaction
+# reciprocal sum: one term of the half sum h.X 5, reduction and sin/cos 5,
+# 35 FMAs 70 -> 80, x 61 = 4.9k.  Contractions: M2L 858, M2P 414, P2L 70
+# (direct kernels: the reference's constants).
 # PP_E pair (cut r < 2, origin separate): 32.5 images x 44 + 30 = 1.46k.
 NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 13100, "CP_E": 12300}
 LEAF_FLOPS = {"PC_D": 581, "PC_E": 7800, "PP_E": 1460}
+# DRAM bytes per interaction of each kernel group, from an ncu capture of the
+# kernels on the 64^3 clustered box at theta 0.2 (dram__bytes_read.sum +
+# dram__bytes_write.sum over the capture's interactions); scaled by this
+# run's counts on the assumption that traffic grows with the interactions.
+TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.3, "CP_E": 6.3}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per interaction of a small capture, "
+                  "scaled by this run's interaction counts")
+
+
+T_START = time.perf_counter()
+
+
+def log(msg):
+    """progress on stderr (the JSON line is the only stdout)"""
+    print("[bench %7.1f s] %s" % (time.perf_counter() - T_START, msg), file=sys.stderr, flush=True)
 
 
 def make_particles(w):
@@ -145,66 +177,100 @@ def reduce_over_ranks(v, op, device):
     return float(t.item())
 
 
-def cpu_reference(x, theta, nthreads, budget_s=1.5, seed=1, walked=None):
-    """Host time of one force evaluation with the reference's kernels (see the
-    module docstring).  walked = (oracle, walk seconds) reuses a finished walk.
-    Returns a dict with the seconds and how they were made."""
+# ---------------------------------------------------------------- CPU side --
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    kind = "reference" if O.ref_lib() is not None else "port"
-    if walked is None:
-        o = O.Oracle(theta=theta, ewald=True, leaf_max=64).set_particles(x)
-        t0 = time.perf_counter()
-        o.build().multipoles().walk()
-        t_walk = time.perf_counter() - t0
-    else:
-        o, t_walk = walked
-    _, counts, _ = o.stats()
+    return O
+
+
+def cpu_walk(x, theta, nthreads):
+    """The reference's tree build, multipoles (serial restatement, timed) and
+    walk (restated kick_fmm on nthreads threads, timed).  Returns the oracle
+    and the seconds of each part."""
+    O = _oracle()
+    o = O.Oracle(theta=theta, ewald=True, leaf_max=64).set_particles(x)
+    t0 = time.perf_counter()
+    o.build().multipoles()
     t1 = time.perf_counter()
+    o.walk(nthreads=nthreads)
+    t2 = time.perf_counter()
+    return o, {"build_multipoles_s": t1 - t0, "walk_s": t2 - t1}
+
+
+def cpu_estimate(o, parts, nthreads, budget_s, seed):
+    """Seconds of one evaluation on the host: the timed tree and walk plus,
+    per kind, this evaluation's interaction count x the reference kernel's
+    sampled host throughput (all nthreads threads)."""
+    O = _oracle()
+    kind = "reference" if O.ref_lib() is not None else "port"
+    _, counts, _ = o.stats()
     costs = o.kind_costs(use_ref=(kind == "reference"), nthreads=nthreads, budget_s=budget_s, seed=seed)
-    t_sample = time.perf_counter() - t1
     t_kern = sum(counts[k] * costs[k][0] * 1e-9 for k in KINDS)
-    return {"seconds": t_walk / nthreads + t_kern, "walk_serial_s": t_walk, "kernels_s": t_kern, "kind": kind,
-            "sample_s": t_sample, "ns_per_interaction": {k: costs[k][0] for k in KINDS},
-            "sampled_interactions": {k: costs[k][1] for k in KINDS}, "counts": counts, "oracle": o}
+    return {"seconds": parts["build_multipoles_s"] + parts["walk_s"] + t_kern, "kernels_s": t_kern, "kind": kind,
+            "ns_per_interaction": {k: costs[k][0] for k in KINDS},
+            "sampled_interactions": {k: int(costs[k][1]) for k in KINDS}, **parts}
 
 
 def cpu_line(r, n, nth, budget_s):
     v = n / r["seconds"] / 1e6
     return {"value": v, "unit": "Mparticles/s", "cores": nth, "kind": r["kind"],
-            "sample": "each of the 8 reference kernels run alone over random sinks of this workload for <=%g s "
-                      "(%d interactions sampled), scaled by this evaluation's interaction counts; plus the serial "
-                      "oracle tree+walk (%.1f s) / %d threads; extrapolated" % (
-                          budget_s, sum(r["sampled_interactions"].values()), r["walk_serial_s"], nth),
+            "sample": "tree build + multipoles (serial, %.1f s) and walk (%d threads, %.1f s) timed in full; each of "
+                      "the 8 reference kernels run over random sinks of this workload with their lists for <=%g s "
+                      "(%d interactions sampled), scaled by this evaluation's interaction counts (%.0f s)" % (
+                          r["build_multipoles_s"], nth, r["walk_s"], budget_s,
+                          sum(r["sampled_interactions"].values()), r["kernels_s"]),
             "seconds_per_eval": r["seconds"], "ns_per_interaction": r["ns_per_interaction"]}
+
+
+def cpu_full_eval(x, theta, nthreads):
+    """One full evaluation with the reference's kernels on the host: tree,
+    multipoles, walk and every interaction (the reference's own kernels on
+    nthreads threads), timed end to end."""
+    O = _oracle()
+    use_ref = O.ref_lib() is not None
+    t0 = time.perf_counter()
+    o = O.Oracle(theta=theta, ewald=True, leaf_max=64).set_particles(x)
+    o.build().multipoles().walk(nthreads=nthreads)
+    o.evaluate(use_ref=use_ref, nthreads=nthreads)
+    sec = time.perf_counter() - t0
+    return {"seconds": sec, "mparticles_per_s": len(x) / sec / 1e6, "theta": theta, "n": int(len(x)),
+            "kind": "reference" if use_ref else "port", "cores": nthreads}
 
 
 def reference_arm(args, w, cfg):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from tigergrav_b200 import ics
     x = make_particles(w)
     n = len(x)
     nth = os.cpu_count() or 1
-    times, last, walked = [], None, None
+    o, parts = cpu_walk(x, args.theta, nth)  # the walk is deterministic: timed once, in full
+    times, last = [], None
     for it in range(args.warmup + args.steps):
-        r = cpu_reference(x, args.theta, nth, budget_s=1.0, seed=1 + it, walked=walked)
-        walked = (r["oracle"], r["walk_serial_s"])  # the walk is deterministic: timed once, reused
+        r = cpu_estimate(o, parts, nth, budget_s=0.5, seed=1 + it)
         if it >= args.warmup:
             times.append(r["seconds"])
         last = r
+    del o
     sec = float(np.mean(times))
     v = n / sec / 1e6
-    cb = cpu_line(last, n, nth, 1.0)
+    cb = cpu_line(last, n, nth, 0.5)
     cb["value"] = v
+    full = {"uniform32_theta0.7": cpu_full_eval(ics.uniform(32768, 1), 0.7, nth),
+            "clustered128_theta0.7": cpu_full_eval(ics.clustered(128, 2), 0.7, nth)}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mparticles/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 sums)", "data": "synthetic (seeded)",
-            "config": cfg, "cpu_baseline": cb,
+            "config": cfg, "cpu_baseline": cb, "measured_full": full,
             "e2e": {"value": v, "unit": "Mparticles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
+
+# ---------------------------------------------------------------- GPU side --
 
 def timed_steps(s, stream, flush, steps, warmup, dt, clock_dev=None):
     """KDK steps with events around each; returns (per-step ms, launches, clocks, stats per step)."""
@@ -240,18 +306,187 @@ def timed_steps(s, stream, flush, steps, warmup, dt, clock_dev=None):
     return [a.elapsed_time(b) for a, b in ev], launches, (clk.summary() if clk else None), stats
 
 
-def force_error(s, x, n, stream):
-    from tigergrav_b200 import ics
-    smp = ics.samples(n, 4096, 3)
+def eval_ms(s, x, stream, flush, reps):
+    """Device time of force evaluations (solve_gravity alone) at positions x."""
+    import torch
+    out = []
     s.set_particles(x)
-    s.solve_gravity(stream=stream)
-    phi, g = s.get_forces()
-    tphi, tgr = s.truth(smp)
+    for k in range(reps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.solve_gravity(stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def truth_at(s, x, smp):
+    s.set_particles(x)
+    return s.truth(smp)
+
+
+def error_vs(g, smp, tgr):
     e = np.linalg.norm(g[smp] - tgr, axis=1) / np.linalg.norm(tgr, axis=1)
     nw = np.sqrt(np.mean(np.sum((g[smp] - tgr) ** 2, 1)) / np.mean(np.sum(tgr ** 2, 1)))
     return {"rms": float(np.sqrt(np.mean(e ** 2))), "max": float(e.max()), "median": float(np.median(e)),
             "normwise": float(nw), "samples": int(len(smp)),
             "definition": "per-particle |g - g_true| / |g_true| at 4096 seeded samples, FP64 direct Ewald truth"}
+
+
+def forces_at(s, x, stream):
+    s.set_particles(x)
+    s.solve_gravity(stream=stream)
+    return s.get_forces()
+
+
+def e2e_run(s, x, stream, flush, steps):
+    """The evaluation through the public API from page-locked host buffers."""
+    import torch
+    n = len(x)
+    xh = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+    vh = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
+    phi_h = torch.zeros(n, dtype=torch.float32).pin_memory()
+    g_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
+    ms = []
+    for k in range(steps + 1):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.set_particles(xh, vh, stream=stream)
+        s.solve_gravity(stream=stream)
+        s.get_forces(out_phi=phi_h, out_g=g_h, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if k >= 1:  # the first call is a warm-up
+            ms.append(a.elapsed_time(b))
+    return ms
+
+
+def adjoint_run(dev, theta=0.7, fd_samples=32):
+    """The differentiation workload (64^3 clustered, seed 5; 8 steps at
+    dt = 1e-3; L = sum w.x(T), w ~ N(0,1) seed 6): tg_forward / tg_backward
+    times on the FP32 path (host clock around the synchronous calls), and
+    central finite differences of the FP64 path (h = 1e-4) against the FP64
+    backward on 32 coordinates (seed 7).  A coordinate whose +h and -h runs
+    have different interaction lists is skipped (a tree force is piecewise
+    smooth) and counted."""
+    import torch
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x0 = ics.clustered(64, 5)
+    n = len(x0)
+    w = np.random.default_rng(6).standard_normal((n, 3))
+    dt, steps, h = 1e-3, 8, 1e-4
+    res = {"workload": "64^3 clustered (seed 5), 8 KDK steps at dt 1e-3, theta %g, L = sum w.x(T)" % theta}
+    with tg.GravitySolver(n, theta=theta, precision="f32", device=dev) as s:
+        s.set_particles(x0).forward(dt, steps)
+        s.backward(w)
+        fw, bw = [], []
+        for _ in range(3):
+            s.set_particles(x0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.forward(dt, steps)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            s.backward(w)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            fw.append(t1 - t0)
+            bw.append(t2 - t1)
+    res.update({"forward_ms": 1e3 * float(np.median(fw)), "backward_ms": 1e3 * float(np.median(bw)),
+                "precision": "f32", "timing": "host clock around the synchronous calls, median of 3"})
+    res["ratio"] = res["backward_ms"] / res["forward_ms"]
+
+    p2d = ics.pos_to_double
+    xd0 = p2d(x0)
+    with tg.GravitySolver(n, theta=theta, precision="f64", device=dev) as s64:
+        s64.set_particles(x0).forward(dt, steps)
+        gx0, _ = s64.backward(w)
+
+        def loss(xpos):
+            s64.set_particles(xpos).solve_gravity()
+            sig = []
+            for _ in range(steps):
+                s64.kick(0.5 * dt)
+                s64.drift(dt)
+                s64.solve_gravity()
+                s64.kick(0.5 * dt)
+                sig.append(tuple(s64.stats()["counts"].values()))
+            xt, _ = s64.get_particles()
+            disp = (p2d(xt) - xd0 + 0.5) % 1.0 - 0.5
+            return float(np.sum(w * (xd0 + disp))), tuple(sig)
+
+        rng = np.random.default_rng(7)
+        idx = rng.choice(n, fd_samples, replace=False)
+        dims = rng.integers(0, 3, fd_samples)
+        errs, nonid, skipped = [], [], 0
+        for i, d in zip(idx, dims):
+            xp, xm = x0.copy(), x0.copy()
+            xp[i, d] = ics.double_to_pos(np.array([xd0[i, d] + h]))[0]
+            xm[i, d] = ics.double_to_pos(np.array([xd0[i, d] - h]))[0]
+            hh = ((p2d(xp[i, d]) - p2d(xm[i, d]) + 0.5) % 1.0) - 0.5
+            (lp, sp), (lm, sm) = loss(xp), loss(xm)
+            if sp != sm:
+                skipped += 1
+                continue
+            fd = (lp - lm) / hh
+            errs.append(abs(gx0[i, d] - fd) / abs(fd))
+            nonid.append(abs((gx0[i, d] - w[i, d]) - (fd - w[i, d])) / max(abs(fd - w[i, d]), 1e-300))
+    errs = np.array(errs)
+    res["fd"] = {"h": h, "samples": fd_samples, "skipped": skipped, "path": "f64",
+                 "median_rel_err": float(np.median(errs)), "p90_rel_err": float(np.percentile(errs, 90)),
+                 "max_rel_err": float(errs.max()), "non_identity_median_rel_err": float(np.median(nonid))}
+    return res
+
+
+def secondary_run(args, dev, stream, flush):
+    """The 128^3 clustered box (seed 2) at theta 0.2 and at the literal 0.7."""
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.clustered(128, 2)
+    n = len(x)
+    smp = ics.samples(n, 4096, 3)
+    out = {}
+    tphi = tgr = None
+    for theta in (0.2, 0.7):
+        with tg.GravitySolver(n, theta=theta, precision=args.precision, device=dev) as s:
+            if tgr is None:
+                tphi, tgr = truth_at(s, x, smp)
+            _, g = forces_at(s, x, stream)
+            s.solve_gravity(stream=stream)
+            ms, _, _, st = timed_steps(s, stream, flush, 5, 3, args.dt)
+            out["clustered128_theta%g" % theta] = {
+                "theta": theta, "value": n / (float(np.mean(ms)) * 1e-3) / 1e6, "unit": "Mparticles/s",
+                "ms_per_step": float(np.mean(ms)),
+                "phase_ms": {k: float(np.mean([q["ms"][k] for q in st])) for k in st[-1]["ms"]},
+                "force_error_vs_fp64_ewald": error_vs(g, smp, tgr)}
+    return out
+
+
+def roofline(phase_ms, cnt, peak):
+    """FP32 roofline of the kernel with the largest share of the evaluation.
+    achieved = executed FP32 operations (per-interaction counts from the
+    kernel source, FMA = 2) / that kernel's CUDA-event phase time."""
+    leaf_far = max(phase_ms["leaves"] - phase_ms.get("pp", 0.0), 1e-9)
+    kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
+            "k_node + k_node_ewald<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
+            "k_ewald_chunk<float> + k_ewald_reduce + k_leaf (PC/PP Ewald, L2P, PC direct)":
+                (leaf_far, LEAF_FLOPS, "leaf")}
+    name = max(kern, key=lambda k: kern[k][0])
+    ms, fl, tk = kern[name]
+    flops = sum(cnt[k] * v for k, v in fl.items())
+    achieved = flops / (ms * 1e-3) / 1e12
+    traffic = sum(cnt[k] * v for k, v in TRAFFIC[tk].items())
+    return {"kernel": name, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+            "peak_source": "measured FP32 FMA kernel on this GPU (tg_device_fp32_peak); MEASURED_PEAKS.json has no "
+                           "FP32 figure",
+            "flops_per_launch": flops, "flops_per_interaction": fl, "ms_per_launch": ms}
 
 
 def main():
@@ -260,14 +495,17 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="clustered128", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="clustered256", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--theta", type=float, default=None,
                     help="opening angle (default: the workload's theta for RMS error <= 1e-4)")
     ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 Ewald error measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--no-literal", action="store_true", help="skip the theta = 0.7 run")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation workload")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the 128^3 runs")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.theta is None:
@@ -277,11 +515,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    cfg = {"workload": "%s (%s), theta %.2g (%s), Ewald, leaf 64, KDK dt %g" % (
+    cfg = {"workload": "%s (%s), theta %.3g (%s), Ewald, leaf 64, KDK dt %g" % (
         args.workload, w["label"], args.theta,
         ("the batching config's theta" if w["kind"] == "batch" else "RMS force error <= 1e-4 on this workload")
-        if args.theta == w["theta_rms"] else "set by --theta",
-        args.dt), "particles_per_gpu": None, "theta": args.theta, "leaf_max": 64, "precision": args.precision,
+        if args.theta == w["theta_rms"] else "set by --theta", args.dt),
+        "particles_per_gpu": (w["nside"] ** 3 if w["kind"] == "clustered" else w.get("n")),
+        "theta": args.theta, "leaf_max": 64, "precision": args.precision,
         "l2": "256 MB flush between timed steps (untimed)", "parallelism": "replicas x%d" % world}
     if args.impl == "reference":
         if w["kind"] == "batch":
@@ -294,6 +533,7 @@ def main():
 
     import torch
     import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
     from tigergrav_b200.solver import device_fp32_peak
 
     dist = world > 1
@@ -306,7 +546,7 @@ def main():
     torch.cuda.set_device(dev)
     x = make_particles(w)
     n = len(x)
-    cfg["particles_per_gpu"] = n
+    log("particles ready: %d" % n)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -323,30 +563,17 @@ def main():
         tdist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step * 1e-3) / 1e6
+    log("timed steps done: %.1f ms per step" % ms_per_step)
     st = stats[-1]
     phase_ms = {k: float(np.mean([q["ms"][k] for q in stats])) for k in st["ms"]}
 
+    # ---- one force evaluation alone (the unit of the FP32 / FP64 comparison) ----
+    ev32 = eval_ms(s, x, stream, flush, 2)
+
     # ---- end to end through the public API with page-locked host buffers ----
-    xh = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
-    vh = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
-    phi_h = torch.zeros(n, dtype=torch.float32).pin_memory()
-    g_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
-    e2e_ms = []
-    s2 = tg.GravitySolver(n, theta=args.theta, ewald=True, leaf_max=64, precision=args.precision, device=dev)
-    for k in range(args.warmup + args.steps):
-        flush.fill_(float(k))
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        s2.set_particles(xh, vh, stream=stream)
-        s2.solve_gravity(stream=stream)
-        s2.get_forces(out_phi=phi_h, out_g=g_h, stream=stream)
-        b.record(stream)
-        torch.cuda.synchronize()
-        if k >= args.warmup:
-            e2e_ms.append(a.elapsed_time(b))
-    s2.close()
+    e2e_ms = e2e_run(s, x, stream, flush, args.e2e_steps)
     e2e_step = float(np.mean(e2e_ms))
+    log("eval %.1f ms, e2e %.1f ms" % (np.mean(ev32), e2e_step))
     e2e_val = world * n / (e2e_step * 1e-3) / 1e6
     if dist:
         e2e_val = reduce_over_ranks(e2e_val, "min", "cuda")
@@ -364,34 +591,53 @@ def main():
             "vs_baseline": None, "dtype": "f32" if args.precision == "f32" else "f64",
             "data": "synthetic (seeded)", "config": cfg,
             "e2e": {"value": e2e_val, "unit": "Mparticles/s", "h2d_bytes_per_step": int(n * 24),
-                    "d2h_bytes_per_step": int(n * 16), "ms_per_step": e2e_step},
+                    "d2h_bytes_per_step": int(n * 16), "ms_per_step": e2e_step, "steps": len(e2e_ms),
+                    "step": "set_particles (host) + solve_gravity + get_forces (host)"},
             "gpu_launches": int(launches), "roofline": roof, "clocks": clocks,
-            "interactions_per_s": float(sum(cnt.values())) / (ms_per_step * 1e-3)}
+            "interactions_per_s": float(sum(cnt.values())) / (ms_per_step * 1e-3),
+            "eval_ms": float(np.mean(ev32))}
 
+    smp = ics.samples(n, 4096, 3)
+    tgr = None
     if rank == 0 and not args.no_error:
-        line["force_error_vs_fp64_ewald"] = force_error(s, x, n, stream)
+        _, tgr = truth_at(s, x, smp)
+        _, g = forces_at(s, x, stream)
+        line["force_error_vs_fp64_ewald"] = error_vs(g, smp, tgr)
         line["accuracy_met"] = line["force_error_vs_fp64_ewald"]["rms"] <= 1e-4
+        del g
+        log("force error: %s" % line["force_error_vs_fp64_ewald"]["rms"])
     s.close()
 
-    if not args.no_literal and args.theta != 0.7:
-        # the workload at the literal theta = 0.7 (error ~7.5e-2 there)
-        s7 = tg.GravitySolver(n, theta=0.7, ewald=True, leaf_max=64, precision=args.precision, device=dev)
-        s7.set_particles(x)
-        s7.solve_gravity(stream=stream)
-        ms7, _, _, st7 = timed_steps(s7, stream, flush, max(args.steps, 5), args.warmup, args.dt)
-        lit = {"theta": 0.7, "value": world * n / (float(np.mean(ms7)) * 1e-3) / 1e6, "unit": "Mparticles/s",
-               "ms_per_step": float(np.mean(ms7)),
-               "phase_ms": {k: float(np.mean([q["ms"][k] for q in st7])) for k in st7[-1]["ms"]}}
-        if rank == 0 and not args.no_error:
-            lit["force_error_vs_fp64_ewald"] = force_error(s7, x, n, stream)
-        s7.close()
-        line["config_theta_0.7"] = lit
+    if not args.no_fp64 and args.precision == "f32":
+        # the plain FP64 port-equivalent path on the same particles and GPU
+        with tg.GravitySolver(n, theta=args.theta, ewald=True, leaf_max=64, precision="f64", device=dev) as s64:
+            s64.set_particles(x).solve_gravity(stream=stream)  # warm-up (allocations)
+            ev64 = eval_ms(s64, x, stream, flush, 1)
+            fp = {"eval_ms": float(np.mean(ev64)), "value": n / (float(np.mean(ev64)) * 1e-3) / 1e6,
+                  "unit": "Mparticles/s per force evaluation", "theta": args.theta}
+            if tgr is not None:
+                _, g64 = s64.get_forces()
+                fp["force_error_vs_fp64_ewald"] = error_vs(g64, smp, tgr)
+                del g64
+        line["fp64_path"] = fp
+        line["fp32_over_fp64"] = fp["eval_ms"] / line["eval_ms"]
+        log("fp64 path: %.1f ms" % fp["eval_ms"])
+
+    if not args.no_adjoint and rank == 0:
+        line["adjoint"] = adjoint_run(dev)
+        log("adjoint: %s" % line["adjoint"])
+
+    if not args.no_secondary and args.workload != "clustered128" and rank == 0:
+        line["secondary"] = secondary_run(args, dev, stream, flush)
+        log("secondary done")
 
     if rank == 0 and world == 1 and not args.no_cpu:
         nth = os.cpu_count() or 1
-        r = cpu_reference(x, args.theta, nth, budget_s=1.5)
+        o, parts = cpu_walk(x, args.theta, nth)
+        r = cpu_estimate(o, parts, nth, budget_s=1.5, seed=1)
+        del o
         line["cpu_baseline"] = cpu_line(r, n, nth, 1.5)
-        del r
+        log("cpu baseline: %s" % line["cpu_baseline"]["sample"])
     if dist:
         tdist.barrier()
         tdist.destroy_process_group()
@@ -450,36 +696,6 @@ def bench_batch(args, w, cfg):
             "serial_ms": float(np.sum(ser)), "speedup_vs_serial": float(np.sum(ser)) / mps}
     print(json.dumps(line), flush=True)
     return 0
-
-
-# DRAM bytes per interaction of each kernel, from the ncu capture summarised
-# in profiles/ewald_pp_kernels_clustered128_theta03.md (dram__bytes_read.sum +
-# dram__bytes_write.sum over its interactions); scaled by this run's counts,
-# assuming traffic in proportion to interactions (PC_E / CP_E at the rate of
-# PP_E / CC_E, which that capture does not contain).
-TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.3, "CP_E": 6.3}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
-
-
-def roofline(phase_ms, cnt, peak):
-    """FP32 roofline of the kernel with the largest share of the evaluation.
-    achieved = executed FP32 operations (per-interaction counts from the
-    kernel source, FMA = 2) / that kernel's CUDA-event phase time."""
-    leaf_far = max(phase_ms["leaves"] - phase_ms.get("pp", 0.0), 1e-9)
-    kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
-            "k_node + k_node_ewald<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
-            "k_ewald_chunk<float,true> + k_leaf<float,64,false> (PC/PP Ewald chunks, L2P, PC direct)":
-                (leaf_far, LEAF_FLOPS, "leaf")}
-    name = max(kern, key=lambda k: kern[k][0])
-    ms, fl, tk = kern[name]
-    flops = sum(cnt[k] * v for k, v in fl.items())
-    achieved = flops / (ms * 1e-3) / 1e12
-    traffic = sum(cnt[k] * v for k, v in TRAFFIC[tk].items())
-    return {"kernel": name, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": traffic,
-            "traffic_source": "ncu DRAM bytes per interaction at 128^3 theta 0.3, scaled by this run's counts",
-            "peak_source": "measured FP32 FMA kernel on this GPU (tg_device_fp32_peak); MEASURED_PEAKS.json has no "
-                           "FP32 figure",
-            "flops_per_launch": flops, "flops_per_interaction": fl, "ms_per_launch": ms}
 
 
 if __name__ == "__main__":

@@ -52,6 +52,7 @@ def lib():
         L.tgo_set_particles.argtypes = [vp, vp, vp, i64]
         for f in ("tgo_build", "tgo_multipoles", "tgo_walk"):
             getattr(L, f).argtypes = [vp]
+        L.tgo_walk_mt.argtypes = [vp, i32]
         L.tgo_evaluate.argtypes = [vp, i32, i32, vp, i64]
         L.tgo_load_reference.argtypes = [vp, C.c_char_p]
         L.tgo_num_nodes.restype = i64
@@ -271,8 +272,9 @@ class Oracle:
         assert lib().tgo_multipoles(self.h) == 0
         return self
 
-    def walk(self):
-        assert lib().tgo_walk(self.h) == 0
+    def walk(self, nthreads=1):
+        """kick_fmm list generation; nthreads > 1 walks subtrees concurrently (same lists)."""
+        assert (lib().tgo_walk(self.h) if nthreads <= 1 else lib().tgo_walk_mt(self.h, int(nthreads))) == 0
         return self
 
     def evaluate(self, use_ref=False, nthreads=0, leaf_subset=None, fp64=False):

@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <dlfcn.h>
+#include <mutex>
 #include <thread>
 #include <chrono>
 #include <vector>
@@ -480,7 +481,23 @@ inline double near_sep(const double *x) {
     return std::sqrt(d);
 }
 
-void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dlist, std::vector<CheckItem> elist);
+/* interaction_stats of one walk (or of one thread's share of it) */
+struct Tally {
+    uint64_t ref_stats[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t counts[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    void add(const Tally &o) {
+        for (int k = 0; k < 6; k++) ref_stats[k] += o.ref_stats[k];
+        for (int k = 0; k < 8; k++) counts[k] += o.counts[k];
+    }
+};
+/* a node with the check lists its parent handed down */
+struct WalkTask {
+    int32_t node;
+    std::vector<CheckItem> d, e;
+};
+
+void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dlist, std::vector<CheckItem> elist, Tally &T,
+               std::vector<WalkTask> *defer);
 
 } // namespace
 
@@ -705,10 +722,11 @@ int tgo_walk(void *h) {
     for (int k = 0; k < TGO_NLIST; k++) {
         S.lists[k].assign(S.nodes.size(), std::vector<int32_t>());
     }
-    for (int k = 0; k < 6; k++) S.ref_stats[k] = 0;
-    for (int k = 0; k < 8; k++) S.counts[k] = 0;
     std::vector<CheckItem> root = {{0, false}};
-    walk_node(S, 0, root, root);
+    Tally T;
+    walk_node(S, 0, root, root, T, nullptr);
+    for (int k = 0; k < 6; k++) S.ref_stats[k] = T.ref_stats[k];
+    for (int k = 0; k < 8; k++) S.counts[k] = T.counts[k];
     return 0;
 }
 
@@ -719,7 +737,8 @@ namespace {
 /* kick_fmm list generation (src/tree.cpp:378-635).  The per-node criterion
  * keeps the reference's mixed float/double arithmetic: (r_a + r_b) is a
  * float sum, theta_inv and h are doubles. */
-void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vector<CheckItem> echecklist) {
+void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vector<CheckItem> echecklist, Tally &T,
+               std::vector<WalkTask> *defer) {
     const Node &nd = S.nodes[n];
     if (nd.pe - nd.pb == 0) return;
     const double h = S.p.soft_len;
@@ -790,15 +809,15 @@ void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vec
             }
         }
     }
-    S.ref_stats[2] += S.lists[TGO_CC_D][n].size();
-    S.ref_stats[4] += dsource_count;
-    S.counts[4] += S.lists[TGO_CC_D][n].size();
-    S.counts[6] += dsource_count;
+    T.ref_stats[2] += S.lists[TGO_CC_D][n].size();
+    T.ref_stats[4] += dsource_count;
+    T.counts[4] += S.lists[TGO_CC_D][n].size();
+    T.counts[6] += dsource_count;
     if (ewald) {
-        S.ref_stats[3] += S.lists[TGO_CC_E][n].size();
-        S.ref_stats[5] += esource_count;
-        S.counts[5] += S.lists[TGO_CC_E][n].size();
-        S.counts[7] += esource_count;
+        T.ref_stats[3] += S.lists[TGO_CC_E][n].size();
+        T.ref_stats[5] += esource_count;
+        T.counts[5] += S.lists[TGO_CC_E][n].size();
+        T.counts[7] += esource_count;
     }
     for (auto f : dfuts) {
         const int32_t c0 = S.nodes[f].child0;
@@ -811,8 +830,13 @@ void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vec
         next_e.push_back({c0 + 1, false});
     }
     if (!nd.leaf()) {
-        walk_node(S, nd.child0, next_d, next_e);
-        walk_node(S, nd.child0 + 1, next_d, next_e);
+        if (defer) { /* the children become tasks of a parallel walk */
+            defer->push_back({nd.child0, next_d, next_e});
+            defer->push_back({nd.child0 + 1, std::move(next_d), std::move(next_e)});
+            return;
+        }
+        walk_node(S, nd.child0, next_d, next_e, T, nullptr);
+        walk_node(S, nd.child0 + 1, next_d, next_e, T, nullptr);
         return;
     }
     /* leaf drain (src/tree.cpp:530-602) */
@@ -847,10 +871,10 @@ void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vec
         dchecklist.swap(next_d);
         next_d.clear();
     }
-    S.ref_stats[4] += nsink * S.lists[TGO_PC_D][n].size();
-    S.ref_stats[0] += nsink * dsource_count;
-    S.counts[2] += nsink * S.lists[TGO_PC_D][n].size();
-    S.counts[0] += nsink * dsource_count;
+    T.ref_stats[4] += nsink * S.lists[TGO_PC_D][n].size();
+    T.ref_stats[0] += nsink * dsource_count;
+    T.counts[2] += nsink * S.lists[TGO_PC_D][n].size();
+    T.counts[0] += nsink * dsource_count;
     if (ewald) {
         echecklist.swap(next_e);
         next_e.clear();
@@ -881,10 +905,10 @@ void walk_node(Solver &S, int32_t n, std::vector<CheckItem> dchecklist, std::vec
             echecklist.swap(next_e);
             next_e.clear();
         }
-        S.ref_stats[5] += nsink * S.lists[TGO_PC_E][n].size();
-        S.ref_stats[1] += nsink * esource_count;
-        S.counts[3] += nsink * S.lists[TGO_PC_E][n].size();
-        S.counts[1] += nsink * esource_count;
+        T.ref_stats[5] += nsink * S.lists[TGO_PC_E][n].size();
+        T.ref_stats[1] += nsink * esource_count;
+        T.counts[3] += nsink * S.lists[TGO_PC_E][n].size();
+        T.counts[1] += nsink * esource_count;
     }
 }
 
@@ -929,6 +953,36 @@ void parallel_for(int64_t n, int nthreads, F &&fn) {
 } // namespace
 
 extern "C" {
+
+/* kick_fmm list generation on nthreads threads, as the reference runs it
+ * (src/tree.cpp:510-515 forks both children as HPX tasks): the top of the
+ * tree is walked level by level until there are enough subtrees, then the
+ * subtrees are walked concurrently.  Every node's lists are still written by
+ * one task in the serial order, so the lists equal tgo_walk's. */
+int tgo_walk_mt(void *h, int nthreads) {
+    Solver &S = *(Solver *)h;
+    if (nthreads <= 1) return tgo_walk(h);
+    for (int k = 0; k < TGO_NLIST; k++) S.lists[k].assign(S.nodes.size(), std::vector<int32_t>());
+    Tally total;
+    std::vector<WalkTask> frontier;
+    frontier.push_back({0, {{0, false}}, {{0, false}}});
+    while (!frontier.empty() && frontier.size() < (size_t)(64 * nthreads)) {
+        std::vector<WalkTask> next;
+        for (auto &t : frontier) walk_node(S, t.node, std::move(t.d), std::move(t.e), total, &next);
+        frontier.swap(next);
+    }
+    std::mutex mtx;
+    parallel_for((int64_t)frontier.size(), nthreads, [&](int64_t k) {
+        Tally T;
+        WalkTask &t = frontier[k];
+        walk_node(S, t.node, std::move(t.d), std::move(t.e), T, nullptr);
+        std::lock_guard<std::mutex> lk(mtx);
+        total.add(T);
+    });
+    for (int k = 0; k < 6; k++) S.ref_stats[k] = total.ref_stats[k];
+    for (int k = 0; k < 8; k++) S.counts[k] = total.counts[k];
+    return 0;
+}
 
 int tgo_load_reference(void *h, const char *so_path) {
     Solver &S = *(Solver *)h;

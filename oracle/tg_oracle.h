@@ -91,6 +91,8 @@ int tgo_build(void *h);
 int tgo_multipoles(void *h);
 /* kick_fmm list generation (src/tree.cpp:378-635) */
 int tgo_walk(void *h);
+/* the same lists on nthreads threads (subtrees walked concurrently) */
+int tgo_walk_mt(void *h, int nthreads);
 /* Evaluate forces along the lists. use_ref: 0 = restated kernels (reference
  * arithmetic), 1 = the reference's kernels loaded by tgo_load_reference,
  * 2 = restated kernels in FP64.  nthreads >= 1.
