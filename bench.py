@@ -74,12 +74,13 @@ WORKLOADS = {
 METRIC = "Mparticles/s per force eval at RMS err<=1e-4 vs FP64 Ewald; adjoint/fwd cost"
 KINDS = ("PP_D", "PP_E", "PC_D", "PC_E", "CC_D", "CC_E", "CP_D", "CP_E")
 
-# FP32 operations per PP pair in k_pp_f32's inner loop, counted from the
-# source with an FMA as 2: separation 9 (per axis two differences of split
-# coordinates and their sum), r^2 5 (1 mul + 2 fma), min 1, clamp 1,
-# rsqrt 1, 1/r^3 2, phi sum 1, three force FMAs 6 -> 26 (the Kahan fold,
-# ~1.3 per pair, is not counted).
-PP_FLOPS = 26
+# FP32 operations per PP pair in k_pp_leaf's inner loop for far source
+# leaves (nearly all pairs at the headline workload), counted from the source
+# with an FMA as 2: separation 3, r^2 5 (1 mul + 2 fma), rsqrt 1, 1/r^3 2,
+# phi sum 1, three force FMAs 6 -> 18 (near leaves: 6 more for the split
+# separation and 2 for the softening clamp; the Kahan fold, ~1.3 per pair,
+# is not counted).
+PP_FLOPS = 18
 # FP32 operations per interaction of the Ewald and multipole kernels, counted
 # from the source the same way.  One real-space image: separation and r^2 8,
 # rsqrt and powers of 1/r 8, erfc/exp 18, d0..d4 31, the moment sums 120 ->
@@ -473,7 +474,7 @@ def roofline(phase_ms, cnt, peak):
     achieved = executed FP32 operations (per-interaction counts from the
     kernel source, FMA = 2) / that kernel's CUDA-event phase time."""
     leaf_far = max(phase_ms["leaves"] - phase_ms.get("pp", 0.0), 1e-9)
-    kern = {"k_pp_f32 (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
+    kern = {"k_pp_leaf (PP direct)": (phase_ms.get("pp", 0.0), {"PP_D": PP_FLOPS}, "pp"),
             "k_node + k_node_ewald<float> (CC/CP direct + Ewald)": (phase_ms["nodes"], NODE_FLOPS, "nodes"),
             "k_ewald_chunk<float> + k_ewald_reduce + k_leaf (PC/PP Ewald, L2P, PC direct)":
                 (leaf_far, LEAF_FLOPS, "leaf")}

@@ -85,6 +85,7 @@ typedef struct tg_stats {
     double ms_build, ms_multipoles, ms_walk, ms_nodes, ms_leaves, ms_kick_drift;
     int64_t launches;     /* kernels of this library launched on this handle so far */
     double ms_pp;         /* part of ms_leaves spent in the FP32 PP-direct kernel (0 when it is not used) */
+    int64_t device_bytes; /* device memory held by this library's buffers in the process (all handles) */
 } tg_stats;
 
 typedef struct tg_solver tg_solver;
@@ -282,6 +283,11 @@ int tg_batch_leapfrog(tg_batch *b, double dt, int n_steps);
 int tg_batch_get_forces(tg_batch *b, float *phi, float *g, int where);
 
 int tg_get_stats(tg_solver *s, tg_stats *out);
+/* Device memory held by this handle's buffers: one "name bytes" line per
+ * buffer and a "total" line, NUL-terminated, into buf (cap bytes; TG_ERR_SIZE
+ * if it does not fit).  For planning runs against the 180 GB of one GPU; no
+ * counterpart in the reference. */
+int tg_memory_report(tg_solver *s, char *buf, int64_t cap);
 
 /* ---- introspection (parity tests) ----------------------------------- */
 int64_t tg_num_nodes(tg_solver *s);

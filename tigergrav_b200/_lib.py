@@ -43,14 +43,16 @@ class tg_stats(C.Structure):
                 ("walk_retries", C.c_int32), ("ref_stats", C.c_uint64 * 6), ("counts", C.c_uint64 * 8),
                 ("flops", C.c_double), ("ms_build", C.c_double), ("ms_multipoles", C.c_double),
                 ("ms_walk", C.c_double), ("ms_nodes", C.c_double), ("ms_leaves", C.c_double),
-                ("ms_kick_drift", C.c_double), ("launches", C.c_int64), ("ms_pp", C.c_double)]
+                ("ms_kick_drift", C.c_double), ("launches", C.c_int64), ("ms_pp", C.c_double),
+                ("device_bytes", C.c_int64)]
 
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
     "tg_error_string", "tg_version", "tg_create", "tg_destroy", "tg_set_particles", "tg_get_particles",
     "tg_build", "tg_multipoles", "tg_walk", "tg_set_walk_capacity", "tg_forces", "tg_solve_gravity", "tg_get_forces",
-    "tg_get_forces_f64", "tg_kick", "tg_drift", "tg_energy", "tg_leapfrog", "tg_get_stats", "tg_num_nodes",
+    "tg_get_forces_f64", "tg_kick", "tg_drift", "tg_energy", "tg_leapfrog", "tg_get_stats", "tg_memory_report",
+    "tg_num_nodes",
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
     "tg_gravity_CC_ewald", "tg_gravity_CP_direct", "tg_gravity_CP_ewald", "tg_truth", "tg_device_fp32_peak",
@@ -92,6 +94,7 @@ def _load():
     L.tg_energy.argtypes = [vp, vp, vp]
     L.tg_leapfrog.argtypes = [vp, d, i32, vp]
     L.tg_get_stats.argtypes = [vp, P(tg_stats)]
+    L.tg_memory_report.argtypes = [vp, vp, i64]
     L.tg_num_nodes.restype = i64
     L.tg_num_nodes.argtypes = [vp]
     L.tg_get_nodes.argtypes = [vp] + [vp] * 10

@@ -7,6 +7,8 @@
 #include <mutex>
 #include <vector>
 
+#include <string>
+
 #include "tg_solver.cuh"
 
 struct tg_solver {
@@ -673,7 +675,37 @@ int tg_get_stats(tg_solver *s, tg_stats *out) {
         if (S.pp_timed) phase_ms(S, 6, 5, &S.st.ms_pp);
     }
     S.st.launches = S.launches;
+    S.st.device_bytes = (int64_t)g_dev_bytes.load();
     *out = S.st;
+    return TG_OK;
+}
+
+int tg_memory_report(tg_solver *s, char *buf, int64_t cap) {
+    if (!s || !buf || cap < 1) return TG_ERR_ARG;
+    Solver &S = s->S;
+    std::string out;
+    int64_t total = 0;
+    auto add = [&](const char *name, size_t bytes) {
+        if (!bytes) return;
+        total += (int64_t)bytes;
+        out += name;
+        out += " " + std::to_string(bytes) + "\n";
+    };
+#define TG_MEM(b) add(#b, S.b.n * sizeof(*S.b.p))
+    TG_MEM(pos); TG_MEM(pos_alt); TG_MEM(vel); TG_MEM(vel_alt); TG_MEM(acc); TG_MEM(accd); TG_MEM(keys);
+    TG_MEM(keys_alt); TG_MEM(idx); TG_MEM(idx_alt); TG_MEM(cub_tmp); TG_MEM(nd_pb); TG_MEM(nd_pe); TG_MEM(nd_child0);
+    TG_MEM(nd_parent); TG_MEM(nd_flag); TG_MEM(nd_scan); TG_MEM(nd_key); TG_MEM(nd_level); TG_MEM(nd_ms);
+    TG_MEM(nd_r); TG_MEM(nd_rmax); TG_MEM(nd_aabb); TG_MEM(nd_prange); TG_MEM(nd_L); TG_MEM(nd_Lloc);
+    TG_MEM(loff[0]); TG_MEM(llen[0]); TG_MEM(pool[0]); TG_MEM(pool[1]); TG_MEM(pool[2]); TG_MEM(pool[3]);
+    TG_MEM(pool[4]); TG_MEM(pool[5]); TG_MEM(pool[6]); TG_MEM(pool[7]); TG_MEM(nxt_pool[0]); TG_MEM(nxt_pool[1]);
+    TG_MEM(nxt_off[0]); TG_MEM(nxt_len[0]); TG_MEM(scratch); TG_MEM(ew_cnt); TG_MEM(ew_off); TG_MEM(ew_part);
+    TG_MEM(ew_nt); TG_MEM(ew_sf); TG_MEM(ew_tpart); TG_MEM(ck_x); TG_MEM(ck_v); TG_MEM(adj_x); TG_MEM(adj_v);
+    TG_MEM(tid_u); TG_MEM(tid_o); TG_MEM(tid_U); TG_MEM(tid_V); TG_MEM(fof_P); TG_MEM(fof_key); TG_MEM(fof_mem);
+    TG_MEM(fof_pairs); TG_MEM(rung_flag); TG_MEM(rung_scan); TG_MEM(rung_nact);
+#undef TG_MEM
+    out += "total " + std::to_string(total) + "\n";
+    if ((int64_t)out.size() + 1 > cap) return TG_ERR_SIZE;
+    std::memcpy(buf, out.c_str(), out.size() + 1);
     return TG_OK;
 }
 

@@ -14,7 +14,7 @@
  *            PC_direct, PP_direct (source leaves staged in shared memory),
  *            PC_ewald, PP_ewald; -phi_self once (src/gravity.cpp:295).
  *            The FP32 path with leaf_max <= 64 runs it without PP_direct
- *            (into an FP64 buffer) and then k_pp_f32 (tg_pp.cuh), which adds
+ *            (into an FP64 buffer) and then k_pp_leaf (tg_pp2.cuh), which adds
  *            PP_direct and phi_self and writes the float4 result.
  *
  * Precision: T = float (FP32 path: FP32 arithmetic, per-tile FP32 partial
@@ -515,20 +515,22 @@ __device__ __forceinline__ uint32_t warp_max_u(uint32_t v) {
 }
 
 /* offset of Y from Xr: int32 wrap (periodic) or plain difference (free space);
- * mag accumulates the largest magnitude, saturated at 2^30 */
+ * mag accumulates the largest magnitude, saturated at 2^31 (a free-space
+ * offset that does not fit an int32 reads as 2^31) */
 __device__ __forceinline__ int32_t rel_off(int32_t Y, int32_t Xr, bool per, uint32_t &mag) {
     if (per) {
         const int32_t a = (int32_t)((uint32_t)Y - (uint32_t)Xr);
-        mag = max(mag, (uint32_t)abs(a));
+        mag = max(mag, a < 0 ? 0u - (uint32_t)a : (uint32_t)a);
         return a;
     }
     const long long a = (long long)Y - (long long)Xr;
     const unsigned long long aa = (unsigned long long)(a < 0 ? -a : a);
-    mag = max(mag, aa >= (1ull << 30) ? (1u << 30) : (uint32_t)aa);
+    mag = max(mag, aa >= (1ull << 31) ? (1u << 31) : (uint32_t)aa);
     return (int32_t)a;
 }
 
 #include "tg_pp.cuh"
+#include "tg_pp2.cuh"
 #include "tg_ewald_sep.cuh"
 #include "tg_ewald_leaf.cuh"
 
@@ -777,8 +779,8 @@ int gravity_forces(Solver &S, cudaStream_t st) {
                     TG_CUDA(cudaEventRecord(S.ev[6], st));
                     S.pp_timed = true;
                 }
-                k_pp_f32<<<2 * g, 32, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.pos.p, LV,
-                                               S.accd.p, S.acc.p);
+                k_pp_leaf<<<g, PPB_T, 0, st>>>(P, S.idx.p, nleaves, S.nd_pb.p, S.nd_pe.p, S.nd_ms.p, S.nd_aabb.p,
+                                               S.pos.p, LV, S.accd.p, S.acc.p);
             }
         } else {
             if (f64)

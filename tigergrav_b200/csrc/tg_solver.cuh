@@ -18,6 +18,7 @@
  */
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -165,24 +166,35 @@ inline int launched(Solver &S) {
     return TG_OK;
 }
 
+/* device bytes held by every DevBuf of the process (all handles) */
+inline std::atomic<long long> g_dev_bytes{0};
+
 template <class T>
 int ensure(DevBuf<T> &b, size_t count) {
     if (b.n >= count && b.p) return TG_OK;
-    if (b.p) cudaFree(b.p);
+    if (b.p) {
+        cudaFree(b.p);
+        g_dev_bytes -= (long long)(b.n * sizeof(T));
+    }
     b.p = nullptr;
     b.n = 0;
     size_t c = count < 16 ? 16 : count;
     c = c + c / 4;
     if (cudaMalloc(&b.p, c * sizeof(T)) != cudaSuccess) {
         cudaGetLastError();
+        b.p = nullptr;
         return TG_ERR_NOMEM;
     }
     b.n = c;
+    g_dev_bytes += (long long)(c * sizeof(T));
     return TG_OK;
 }
 template <class T>
 void release(DevBuf<T> &b) {
-    if (b.p) cudaFree(b.p);
+    if (b.p) {
+        cudaFree(b.p);
+        g_dev_bytes -= (long long)(b.n * sizeof(T));
+    }
     b.p = nullptr;
     b.n = 0;
 }

@@ -263,8 +263,14 @@ class GravitySolver:
         refk = ("PP_direct", "PP_ewald", "CC_direct", "CC_ewald", "CP_direct", "CP_ewald")
         return dict(n=s.n, nodes=s.nodes, leaves=s.leaves, depth=s.depth, walk_retries=s.walk_retries,
                     ref_stats=dict(zip(refk, map(int, s.ref_stats))), counts=dict(zip(kinds, map(int, s.counts))),
-                    flops=s.flops, launches=s.launches, ms=dict(build=s.ms_build, multipoles=s.ms_multipoles, walk=s.ms_walk,
+                    flops=s.flops, launches=s.launches, device_bytes=s.device_bytes, ms=dict(build=s.ms_build, multipoles=s.ms_multipoles, walk=s.ms_walk,
                                            nodes=s.ms_nodes, leaves=s.ms_leaves, pp=s.ms_pp))
+
+    def memory(self) -> dict:
+        """Device bytes per buffer of this handle (and "total")."""
+        buf = C.create_string_buffer(1 << 16)
+        check("tg_memory_report", lib.tg_memory_report(self.h, buf, len(buf)))
+        return {k: int(v) for k, v in (ln.split() for ln in buf.value.decode().splitlines())}
 
     # ---- introspection ----
     @property
