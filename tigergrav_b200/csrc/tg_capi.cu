@@ -321,6 +321,7 @@ int tg_destroy(tg_solver *s) {
         release(S.nxt_len[q]);
         release(S.nxt_pool[q]);
     }
+    release(S.nx_top);
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
     release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part); release(S.ew_nt); release(S.ew_sf); release(S.ew_tpart);
@@ -429,7 +430,7 @@ int tg_set_walk_capacity(tg_solver *s, int64_t entries) {
     tg::Solver &S = s->S;
     S.cap_start = entries;
     for (int k = 0; k < tg::NLIST; k++) S.list_cap[k] = 0;
-    S.nx_cap = 0;
+    S.nx_cap[0] = S.nx_cap[1] = 0;
     if (entries > 0) S.scratch_per_warp = 0;
     return TG_OK;
 }

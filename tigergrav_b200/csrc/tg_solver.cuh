@@ -77,7 +77,8 @@ struct Solver {
 
     /* nodes */
     int64_t nnodes = 0;
-    std::vector<int64_t> level_off; /* host: first node of each level, size depth+2 */
+    std::vector<int64_t> level_off;    /* host: first node of each level, size depth+2 */
+    std::vector<int64_t> level_leaves; /* host: leaves (childless nodes) of each level, size depth+1 */
     int depth = 0;
     DevBuf<int32_t> nd_pb, nd_pe, nd_child0, nd_parent, nd_flag, nd_scan;
     DevBuf<unsigned long long> nd_key;
@@ -96,12 +97,13 @@ struct Solver {
     DevBuf<unsigned long long> pool_top; /* NLIST + 2 counters */
     DevBuf<int64_t> nxt_off[2];          /* per node: offset of next list (direct, ewald) */
     DevBuf<int32_t> nxt_len[2];
-    DevBuf<int32_t> nxt_pool[2];
+    DevBuf<int32_t> nxt_pool[2];         /* two halves each: even and odd levels */
+    DevBuf<unsigned long long> nx_top;   /* per level: next-list tops (direct, ewald), drain counter, spare */
     DevBuf<int32_t> scratch;             /* leaf drain per-warp scratch */
     int64_t scratch_per_warp = 0;
     int drain_warps = 0;
     int64_t list_cap[NLIST] = {0, 0, 0, 0, 0, 0, 0, 0}; /* pool capacities that served the last walk */
-    int64_t nx_cap = 0;
+    int64_t nx_cap[2] = {0, 0};
     int64_t cap_start = 0; /* tg_set_walk_capacity: first capacity of every pool (0: sized from the tree) */
 
     /* status / stats */

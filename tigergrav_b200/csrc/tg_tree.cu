@@ -163,6 +163,7 @@ int tree_build(Solver &S, cudaStream_t st) {
     TG_TRY(launched(S));
     S.level_off.assign(1, 0);
     S.level_off.push_back(1);
+    S.level_leaves.clear();
     int L = 0;
     for (;;) {
         const int64_t first = S.level_off[L], count = S.level_off[L + 1] - S.level_off[L];
@@ -180,6 +181,7 @@ int tree_build(Solver &S, cudaStream_t st) {
         TG_CUDA(cudaMemcpyAsync(&h2[1], S.nd_flag.p + count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         TG_CUDA(cudaStreamSynchronize(st));
         const int64_t nsplit = (int64_t)h2[0] + h2[1];
+        S.level_leaves.push_back(count - nsplit); /* nodes of this level that stay leaves (empty ones too) */
         if (nsplit == 0) break;
         if (L >= 63) return TG_ERR_DEPTH; /* children would need key bit -1 */
         const int64_t next_first = S.level_off[L + 1];

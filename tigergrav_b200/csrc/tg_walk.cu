@@ -201,8 +201,9 @@ __device__ void node_stage_list(const WalkParams &W, const NodeView &V, bool ewa
 
 __global__ void k_node_stage(WalkParams W, NodeView V, int64_t first, int64_t count, int32_t nnodes,
                              const int32_t *__restrict__ parent, int32_t **pools, const int64_t *caps,
-                             unsigned long long *tops, int64_t **loff, int32_t **llen, int32_t *nx_pool_d,
-                             int32_t *nx_pool_e, int64_t cap_nx, int64_t *nx_off_d, int32_t *nx_len_d,
+                             unsigned long long *tops, int64_t **loff, int32_t **llen, const int32_t *nx_in_d,
+                             const int32_t *nx_in_e, int32_t *nx_out_d, int32_t *nx_out_e, int64_t cap_nx_d,
+                             int64_t cap_nx_e, unsigned long long *nx_top, int64_t *nx_off_d, int32_t *nx_len_d,
                              int64_t *nx_off_e, int32_t *nx_len_e, uint32_t *err) {
     const int lane = threadIdx.x & 31;
     const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -229,18 +230,18 @@ __global__ void k_node_stage(WalkParams W, NodeView V, int64_t first, int64_t co
         nin_d = 1;
         nin_e = W.ewald ? 1 : 0;
     } else {
-        in_d = nx_pool_d + nx_off_d[p];
+        in_d = nx_in_d + nx_off_d[p];
         nin_d = nx_len_d[p];
-        in_e = nx_pool_e + nx_off_e[p];
+        in_e = nx_in_e + nx_off_e[p];
         nin_e = W.ewald ? nx_len_e[p] : 0;
     }
     node_stage_list(W, V, false, X, r, rmax, in_d, nin_d, nnodes, pools[TG_CC_D], caps[TG_CC_D], &tops[TG_CC_D],
                     &loff[TG_CC_D][i], &llen[TG_CC_D][i], pools[TG_CP_D], caps[TG_CP_D], &tops[TG_CP_D],
-                    &loff[TG_CP_D][i], &llen[TG_CP_D][i], nx_pool_d, cap_nx, &tops[NLIST], &nx_off_d[i],
+                    &loff[TG_CP_D][i], &llen[TG_CP_D][i], nx_out_d, cap_nx_d, &nx_top[0], &nx_off_d[i],
                     &nx_len_d[i], err);
     node_stage_list(W, V, true, X, r, rmax, in_e, nin_e, nnodes, pools[TG_CC_E], caps[TG_CC_E], &tops[TG_CC_E],
                     &loff[TG_CC_E][i], &llen[TG_CC_E][i], pools[TG_CP_E], caps[TG_CP_E], &tops[TG_CP_E],
-                    &loff[TG_CP_E][i], &llen[TG_CP_E][i], nx_pool_e, cap_nx, &tops[NLIST + 1], &nx_off_e[i],
+                    &loff[TG_CP_E][i], &llen[TG_CP_E][i], nx_out_e, cap_nx_e, &nx_top[1], &nx_off_e[i],
                     &nx_len_e[i], err);
 }
 
@@ -349,9 +350,9 @@ __device__ void drain_list(const WalkParams &W, const NodeView &V, bool ewald_li
     for (int j = lane; j < n_pc; j += 32) pool_pc[b_pc + j] = outPC[j];
 }
 
-__global__ void k_leaf_drain(WalkParams W, NodeView V, const int32_t *__restrict__ leaves, int32_t nleaves,
-                             int32_t nnodes, int32_t **pools, const int64_t *caps, unsigned long long *tops,
-                             int64_t **loff, int32_t **llen, const int32_t *nx_pool_d, const int32_t *nx_pool_e,
+__global__ void k_leaf_drain(WalkParams W, NodeView V, int64_t first, int64_t count, int32_t nnodes,
+                             int32_t **pools, const int64_t *caps, unsigned long long *tops, int64_t **loff,
+                             int32_t **llen, const int32_t *nx_pool_d, const int32_t *nx_pool_e,
                              const int64_t *nx_off_d, const int32_t *nx_len_d, const int64_t *nx_off_e,
                              const int32_t *nx_len_e, int32_t *scratch, int64_t scr_cap,
                              unsigned long long *work_counter, uint32_t *err) {
@@ -359,11 +360,13 @@ __global__ void k_leaf_drain(WalkParams W, NodeView V, const int32_t *__restrict
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int32_t *scr = scratch + warp * 4 * scr_cap;
     for (;;) {
-        int32_t k = 0;
-        if (lane == 0) k = (int32_t)atomicAdd(work_counter, 1ull);
+        int64_t k = 0;
+        if (lane == 0) k = (int64_t)atomicAdd(work_counter, 1ull);
         k = __shfl_sync(0xffffffffu, k, 0);
-        if (k >= nleaves) break;
-        const int32_t i = leaves[k];
+        if (k >= count) break;
+        const int32_t i = (int32_t)(first + k);
+        /* the leaves of this level with (active) particles */
+        if (V.child0[i] >= 0 || V.pe[i] == V.pb[i] || (W.nact && W.nact[i] == 0)) continue;
         const MSrc &s = V.ms[i];
         const double X[3] = {pos2d(s.x[0]), pos2d(s.x[1]), pos2d(s.x[2])};
         const float r = V.r[i], rmax = V.rmax[i];
@@ -446,7 +449,7 @@ int tree_walk(Solver &S, cudaStream_t st) {
     /* capacities: those that served the last walk, else sized from the tree;
      * on an overflow the pools grow to the totals the walk asked for */
     int64_t cap[NLIST];
-    int64_t cap_nx = 0;
+    int64_t cap_nx[2] = {0, 0};
     {
         const int64_t base_nodes = nn + 64;
         const int64_t base_leaves = nleaves + 64;
@@ -460,15 +463,23 @@ int tree_walk(Solver &S, cudaStream_t st) {
                                      (S.prm.ewald ? 32 : 1) * base_leaves};
         for (int k = 0; k < NLIST; k++)
             cap[k] = S.cap_start > 0 ? S.cap_start : (S.list_cap[k] > 0 ? S.list_cap[k] : dflt[k]);
-        cap_nx = S.cap_start > 0 ? S.cap_start : (S.nx_cap > 0 ? S.nx_cap : 400 * base_nodes);
+        /* the next lists of one level: a few hundred entries per node of the widest level */
+        int64_t widest = 1;
+        for (int L = 0; L <= S.depth; L++) widest = std::max(widest, S.level_off[L + 1] - S.level_off[L]);
+        const int64_t dflt_nx[2] = {256 * widest + 4096, (S.prm.ewald ? 64 : 1) * widest + 4096};
+        for (int q = 0; q < 2; q++)
+            cap_nx[q] = S.cap_start > 0 ? S.cap_start : (S.nx_cap[q] > 0 ? S.nx_cap[q] : dflt_nx[q]);
         if (S.scratch_per_warp == 0) S.scratch_per_warp = 4096;
         if (S.cap_start > 0) S.scratch_per_warp = std::min<int64_t>(S.scratch_per_warp, S.cap_start);
     }
     int tries = 0;
+    const int nlev = S.depth + 1;
     for (;;) {
         for (int k = 0; k < NLIST; k++) TG_TRY(ensure(S.pool[k], cap[k]));
-        TG_TRY(ensure(S.nxt_pool[0], cap_nx));
-        TG_TRY(ensure(S.nxt_pool[1], S.prm.ewald ? cap_nx : 16));
+        /* next lists: two halves per kind, the levels alternate between them */
+        TG_TRY(ensure(S.nxt_pool[0], 2 * (size_t)cap_nx[0]));
+        TG_TRY(ensure(S.nxt_pool[1], 2 * (size_t)cap_nx[1]));
+        TG_TRY(ensure(S.nx_top, 2 * (size_t)nlev + 2 * (size_t)nlev));
         S.drain_warps = S.num_sms * 16;
         TG_TRY(ensure(S.scratch, (size_t)S.drain_warps * 4 * S.scratch_per_warp));
         int32_t *h_pools[NLIST], *h_llen[NLIST];
@@ -482,8 +493,9 @@ int tree_walk(Solver &S, cudaStream_t st) {
         TG_CUDA(cudaMemcpyAsync(d_llen.p, h_llen, sizeof(h_llen), cudaMemcpyHostToDevice, st));
         TG_CUDA(cudaMemcpyAsync(d_loff.p, h_loff, sizeof(h_loff), cudaMemcpyHostToDevice, st));
         TG_CUDA(cudaMemcpyAsync(d_caps.p, cap, sizeof(cap), cudaMemcpyHostToDevice, st));
-        TG_CUDA(cudaMemsetAsync(S.pool_top.p, 0, sizeof(unsigned long long) * (NLIST + 2), st));
-        TG_CUDA(cudaMemsetAsync(S.pool_top.p + NLIST + 3, 0, sizeof(unsigned long long), st));
+        TG_CUDA(cudaMemsetAsync(S.pool_top.p, 0, sizeof(unsigned long long) * NLIST, st));
+        /* per level: next-list tops (direct, ewald) and the drain's work counter */
+        TG_CUDA(cudaMemsetAsync(S.nx_top.p, 0, sizeof(unsigned long long) * 4 * nlev, st));
         TG_CUDA(cudaMemsetAsync(S.dev_err.p, 0, sizeof(uint32_t), st));
         {
             const int g = (int)((nn + 255) / 256);
@@ -493,22 +505,30 @@ int tree_walk(Solver &S, cudaStream_t st) {
         for (int L = 0; L <= S.depth; L++) {
             const int64_t first = S.level_off[L], count = S.level_off[L + 1] - S.level_off[L];
             if (count <= 0) continue;
-            const int TPB = 128;
-            const int g = (int)((count * 32 + TPB - 1) / TPB);
-            k_node_stage<<<g, TPB, 0, st>>>(W, V, first, count, (int32_t)nn, S.nd_parent.p, d_pools.p, d_caps.p,
-                                            S.pool_top.p, d_loff.p, d_llen.p, S.nxt_pool[0].p, S.nxt_pool[1].p, cap_nx,
-                                            S.nxt_off[0].p, S.nxt_len[0].p, S.nxt_off[1].p, S.nxt_len[1].p,
-                                            S.dev_err.p);
-            TG_TRY(launched(S));
-        }
-        if (nleaves > 0) {
-            const int TPB = 128;
-            const int g = S.drain_warps * 32 / TPB;
-            k_leaf_drain<<<g, TPB, 0, st>>>(W, V, S.idx.p, nleaves, (int32_t)nn, d_pools.p, d_caps.p, S.pool_top.p,
-                                            d_loff.p, d_llen.p, S.nxt_pool[0].p, S.nxt_pool[1].p, S.nxt_off[0].p,
-                                            S.nxt_len[0].p, S.nxt_off[1].p, S.nxt_len[1].p, S.scratch.p,
-                                            S.scratch_per_warp, S.pool_top.p + NLIST + 3, S.dev_err.p);
-            TG_TRY(launched(S));
+            const size_t in_h = (size_t)((L + 1) & 1), out_h = (size_t)(L & 1);
+            int32_t *const nd_in = S.nxt_pool[0].p + in_h * cap_nx[0], *const ne_in = S.nxt_pool[1].p + in_h * cap_nx[1];
+            int32_t *const nd_out = S.nxt_pool[0].p + out_h * cap_nx[0];
+            int32_t *const ne_out = S.nxt_pool[1].p + out_h * cap_nx[1];
+            unsigned long long *const lt = S.nx_top.p + 4 * (size_t)L; /* direct, ewald, drain counter */
+            {
+                const int TPB = 128;
+                const int g = (int)((count * 32 + TPB - 1) / TPB);
+                k_node_stage<<<g, TPB, 0, st>>>(W, V, first, count, (int32_t)nn, S.nd_parent.p, d_pools.p, d_caps.p,
+                                                S.pool_top.p, d_loff.p, d_llen.p, nd_in, ne_in, nd_out, ne_out,
+                                                cap_nx[0], cap_nx[1], lt, S.nxt_off[0].p, S.nxt_len[0].p,
+                                                S.nxt_off[1].p, S.nxt_len[1].p, S.dev_err.p);
+                TG_TRY(launched(S));
+            }
+            if (S.level_leaves[L] > 0) { /* drain this level's leaves while their next lists are live */
+                const int TPB = 128;
+                const int64_t want = std::min<int64_t>(S.drain_warps, S.level_leaves[L]);
+                const int g = (int)((want * 32 + TPB - 1) / TPB);
+                k_leaf_drain<<<g, TPB, 0, st>>>(W, V, first, count, (int32_t)nn, d_pools.p, d_caps.p, S.pool_top.p,
+                                                d_loff.p, d_llen.p, nd_out, ne_out, S.nxt_off[0].p, S.nxt_len[0].p,
+                                                S.nxt_off[1].p, S.nxt_len[1].p, S.scratch.p, S.scratch_per_warp,
+                                                lt + 2, S.dev_err.p);
+                TG_TRY(launched(S));
+            }
         }
         uint32_t err = 0;
         TG_TRY(read_err(S, st, &err));
@@ -528,24 +548,29 @@ int tree_walk(Solver &S, cudaStream_t st) {
             return TG_ERR_CAPACITY;
         }
         /* the pool tops kept counting past a full pool: they are what this
-         * walk asked for (a lower bound when a next-list or scratch overflow
-         * starved the levels below, hence at least doubling then) */
-        unsigned long long tops[NLIST + 2];
-        TG_CUDA(cudaMemcpyAsync(tops, S.pool_top.p, sizeof(tops), cudaMemcpyDeviceToHost, st));
+         * walk asked for, unless a next-list or scratch overflow starved the
+         * levels below (then the lists keep their size until a walk that is
+         * not starved has counted them, and the next lists at least double) */
+        std::vector<unsigned long long> tops(NLIST), ltops(4 * (size_t)nlev);
+        TG_CUDA(cudaMemcpyAsync(tops.data(), S.pool_top.p, sizeof(unsigned long long) * NLIST, cudaMemcpyDeviceToHost,
+                                st));
+        TG_CUDA(cudaMemcpyAsync(ltops.data(), S.nx_top.p, sizeof(unsigned long long) * 4 * nlev,
+                                cudaMemcpyDeviceToHost, st));
         TG_CUDA(cudaStreamSynchronize(st));
         const bool starved = (err & (DEV_ERR_OVERFLOW_NEXT | DEV_ERR_OVERFLOW_SCRATCH)) != 0;
-        for (int k = 0; k < NLIST; k++) {
-            const int64_t want = (int64_t)tops[k] + (int64_t)(tops[k] / 8) + 1024;
-            if ((int64_t)tops[k] > cap[k]) cap[k] = std::max(want, starved ? 2 * cap[k] : want);
-        }
-        if (err & DEV_ERR_OVERFLOW_NEXT) {
-            const int64_t t = (int64_t)std::max(tops[NLIST], tops[NLIST + 1]);
-            cap_nx = std::max(2 * cap_nx, t + t / 8 + 1024);
+        if (!starved)
+            for (int k = 0; k < NLIST; k++)
+                if ((int64_t)tops[k] > cap[k]) cap[k] = (int64_t)tops[k] + (int64_t)(tops[k] / 8) + 1024;
+        for (int q = 0; q < 2; q++) {
+            int64_t t = 0;
+            for (int L = 0; L < nlev; L++) t = std::max<int64_t>(t, (int64_t)ltops[4 * (size_t)L + q]);
+            if (t > cap_nx[q]) cap_nx[q] = std::max(2 * cap_nx[q], t + t / 8 + 1024);
         }
         if (err & DEV_ERR_OVERFLOW_SCRATCH) S.scratch_per_warp *= 2;
     }
     for (int k = 0; k < NLIST; k++) S.list_cap[k] = cap[k];
-    S.nx_cap = cap_nx;
+    S.nx_cap[0] = cap_nx[0];
+    S.nx_cap[1] = cap_nx[1];
     S.st.walk_retries = tries;
     S.st.leaves = nleaves;
     release(d_pools);
