@@ -129,6 +129,34 @@ def ref_lib():
     return _ref
 
 
+_ref_copies = {}
+_ref_tmpdir = None
+
+
+def ref_path_for(theta, soft_len, m_tot, n, ewald, G) -> str:
+    """Path of a copy of the reference's kernel library to load for these
+    options.  The reference's kernels keep the options of their first call in
+    function-local statics (src/gravity.cpp:176-187, 307-312, 375-378), so
+    one loaded library serves one parameter set per process: every further
+    parameter set gets its own copy of the file, loaded separately."""
+    global _ref_tmpdir
+    key = (float(theta), float(soft_len), float(m_tot), int(n), int(ewald), float(G))
+    if key not in _ref_copies:
+        if not _ref_copies:
+            _ref_copies[key] = REF_PATH
+        else:
+            import atexit
+            import shutil
+            import tempfile
+            if _ref_tmpdir is None:
+                _ref_tmpdir = tempfile.mkdtemp(prefix="tg_ref_")
+                atexit.register(shutil.rmtree, _ref_tmpdir, True)
+            path = os.path.join(_ref_tmpdir, "libtg_ref_%d.so" % len(_ref_copies))
+            shutil.copyfile(REF_PATH, path)
+            _ref_copies[key] = path
+    return _ref_copies[key]
+
+
 def _p(a):
     return None if a is None else a.ctypes.data
 
@@ -277,12 +305,16 @@ class Oracle:
         assert (lib().tgo_walk(self.h) if nthreads <= 1 else lib().tgo_walk_mt(self.h, int(nthreads))) == 0
         return self
 
+    def _ref_path(self):
+        p = self.p
+        return ref_path_for(p.theta, p.soft_len, p.m * self.n, self.n, p.ewald, p.G)
+
     def evaluate(self, use_ref=False, nthreads=0, leaf_subset=None, fp64=False):
         """use_ref: the reference's own kernels; fp64: the restated kernels in double."""
         if use_ref:
             if ref_lib() is None:
                 raise RuntimeError("reference kernels not built (oracle/_ref)")
-            rc = lib().tgo_load_reference(self.h, REF_PATH.encode())
+            rc = lib().tgo_load_reference(self.h, self._ref_path().encode())
             if rc != 0:
                 raise RuntimeError("tgo_load_reference: %d" % rc)
         nt = nthreads or os.cpu_count() or 1
@@ -349,7 +381,7 @@ class Oracle:
         if use_ref:
             if ref_lib() is None:
                 raise RuntimeError("reference kernels not built (oracle/_ref)")
-            rc = lib().tgo_load_reference(self.h, REF_PATH.encode())
+            rc = lib().tgo_load_reference(self.h, self._ref_path().encode())
             if rc != 0:
                 raise RuntimeError("tgo_load_reference: %d" % rc)
         ns = np.zeros(8)

@@ -15,3 +15,33 @@ def leaf_members(nodes, perm):
         if e > b:
             out[int(nodes["boxid"][i])] = np.sort(perm[b:e])
     return out
+
+
+# The FP32 parity bound: per particle, the path may be no further from the
+# FP64 evaluation of the same interaction lists than the reference's own FP32
+# arithmetic is, plus 1e-5 of the force.  A force far below the rms force is
+# the cancellation of much larger partial sums, whose FP32 rounding sets its
+# error in any summation order (at 128^3, theta 0.7, the reference's kernels
+# and their restatement, which differ only in order, deviate by 7e-6 and
+# 2.8e-5 of |g| = 0.12 g_rms at one particle), so the 1e-5 applies to
+# max(|g|, g_rms / 4).  The potential takes 1e-5 of |phi| with a floor of
+# 1e-6 of the rms potential (periodic potentials cross zero).
+ARBITER_REL = 1e-5
+ARBITER_G_FLOOR = 0.25
+ARBITER_PHI_FLOOR = 1e-6
+
+
+def arbiter_excess(g, g_ref, g64, phi=None, phi_ref=None, phi64=None):
+    """Largest violation of |x - x64| <= |x_ref - x64| + tol over the particles,
+    in units of the tolerance term (<= 0 everywhere: the bound holds).
+    Returns (force excess, potential excess or None)."""
+    n64 = np.linalg.norm(g64, axis=1)
+    scale = np.maximum(n64, ARBITER_G_FLOOR * np.sqrt(np.mean(n64 ** 2)))
+    lhs = np.linalg.norm(g - g64, axis=1)
+    rhs = np.linalg.norm(g_ref - g64, axis=1) + ARBITER_REL * scale
+    fx = float(np.max((lhs - rhs) / np.maximum(ARBITER_REL * scale, 1e-300)))
+    if phi is None:
+        return fx, None
+    tol = ARBITER_REL * np.abs(phi64) + ARBITER_PHI_FLOOR * np.sqrt(np.mean(phi64 ** 2))
+    px = float(np.max((np.abs(phi - phi64) - np.abs(phi_ref - phi64) - tol) / tol))
+    return fx, px
