@@ -82,7 +82,8 @@ typedef struct tg_stats {
     uint64_t counts[8];
     double flops;         /* reference flop convention (src/gravity.cpp:299-784, tree.cpp:234) */
     /* device time of the last solve, per phase, milliseconds */
-    double ms_build, ms_multipoles, ms_walk, ms_nodes, ms_leaves, ms_kick_drift;
+    double ms_build, ms_multipoles, ms_walk, ms_nodes, ms_leaves;
+    double ms_kick_drift; /* the tg_kick_drift right before the last solve, if there was one */
     int64_t launches;     /* kernels of this library launched on this handle so far */
     double ms_pp;         /* part of ms_leaves spent in the FP32 PP-direct kernel (0 when it is not used) */
     int64_t device_bytes; /* device memory held by this library's buffers in the process (all handles) */
@@ -151,7 +152,17 @@ int tg_energy(tg_solver *s, double out[5], void *stream);
 #define TG_NOALLOC_MAX_N (1ll << 26)
 int tg_energy_noalloc(const float *v, const float *phi, int64_t n, double m, double G, double *out,
                       int device, void *stream);
-/* n_steps kick-drift-kick leapfrog steps of dt (first call computes forces if needed). */
+/* The kick that closes one step, the kick that opens the next and the drift
+ * between them in one pass over the particles: v += g G dt_close, v += g G
+ * dt_open (each product rounded to float and added as tg_kick does; dt_close
+ * = 0 skips the first), then x = wrap(x + v dt_drift) as tg_drift.  The
+ * reference fuses its kick into the force stage (src/tree.cpp:630) and
+ * drifts in a separate pass (part_vect_drift, src/part_vect.cpp:493-540).
+ * Needs forces; like tg_drift it invalidates the tree. */
+int tg_kick_drift(tg_solver *s, double dt_close, double dt_open, double dt_drift, void *stream);
+/* n_steps kick-drift-kick leapfrog steps of dt (first call computes forces if
+ * needed); between steps the closing and opening kicks and the drift run as
+ * one tg_kick_drift, with the same arithmetic as kick, drift, solve, kick. */
 int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream);
 
 /* ---- differentiation (forward/backward pair, like torch.autograd.Function) ----
@@ -259,6 +270,29 @@ typedef struct {
     double t;           /* itime in units of time */
 } tg_rung_state;
 int tg_rung_step(tg_solver *s, const tg_rung_params *p, tg_rung_state *state, int all_forces, void *stream);
+/* The same step with the reference's cosmological factors (opts.cosmic):
+ * before the drift, cosmo_advance (src/cosmo.cpp:187-218) moves the expansion
+ * by the step of the largest rung (time accumulated in float, as the
+ * reference's this_time) and gives, per rung, kick_dt1 (back over half the
+ * rung's step; kept from earlier steps until the time reaches the step) and
+ * kick_dt2 (ahead over half the step), and the drift factor over the step.
+ * The kick (src/part_vect.cpp:358-381) closes with kick_dt1 of the old rung,
+ * chooses the rung from |g G| / a^3 with a the scale factor at the start of
+ * the step, and opens with kick_dt2 of the stored rung (the fixed check:
+ * opts.cosmic where the reference tests opts.ewald, src/part_vect.cpp:376).
+ * tg_cosmo_rung_init starts a state at scale factor a and da/dt adot (the
+ * reference starts at a = 1, adot = H0: cosmos::cosmos, src/cosmo.cpp:29-37).
+ * *cs changes only when the step succeeds. */
+typedef struct {
+    double a, adot, tau; /* the expansion now (this_cosmos) */
+    double a_last;       /* the scale factor at the start of the last step (last_cosmos) */
+    float time;          /* the reference's float time accumulator (this_time) */
+    int32_t reserved;
+    double kick1[31];    /* kick_dt1 per rung, kept between steps like the reference's array */
+} tg_cosmo_rung_state;
+int tg_cosmo_rung_init(tg_cosmo_rung_state *cs, double a, double adot);
+int tg_rung_step_cosmo(tg_solver *s, const tg_rung_params *p, tg_rung_state *state, const tg_cosmo_params *cp,
+                       tg_cosmo_rung_state *cs, int all_forces, void *stream);
 int tg_get_rungs(tg_solver *s, int8_t *rung, int where, void *stream);
 int tg_group_catalog(tg_solver *s, double a, double *out, int64_t capacity, int64_t *ngroups, void *stream);
 

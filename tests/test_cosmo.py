@@ -19,8 +19,9 @@ def test_matches_restatement_lcdm():
     for dt in (0.01, 0.02, 0.05):
         s_lib, f_lib = cosmo_kdk(s_lib, dt, H0, om, ol)
         s_or, f_or = oc.kdk_factors(s_or, dt, H0, om, ol)
-        assert np.allclose(s_lib, s_or, rtol=1e-13, atol=0)
-        assert np.allclose(f_lib, f_or, rtol=1e-13, atol=0)
+        # the same operations in the same order: bit for bit
+        assert list(s_lib) == list(s_or)
+        assert list(f_lib) == list(f_or)
 
 
 def test_einstein_de_sitter():
@@ -32,3 +33,24 @@ def test_einstein_de_sitter():
     assert abs(f[1] - 3 * (1 - 1.1 ** (-1 / 3))) < 1e-12
     assert abs(f[2] - 3 * (1.1 ** (1 / 3) - 1.05 ** (1 / 3))) < 1e-12
     assert abs(st[2] - 3 * (1.1 ** (1 / 3) - 1)) < 1e-12  # tau = int dt / a
+
+
+def test_rung_advance_factors():
+    """the oracle's cosmo_advance for rung steps: kick_dt1 is filled only once
+    the float time reaches a rung's step; the factors integrate 1/a over half
+    steps (Einstein-de Sitter: closed forms)"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cosmo as oc
+    t_max = 0.25
+    cs = oc.rung_state(1.0, 2.0 / 3.0)  # EdS, t = 1 at a = 1
+    drift, k1, k2, a3inv = oc.rung_advance(cs, 0.0, t_max, 2.0 / 3.0, 1.0, 0.0)
+    assert drift == 0.0 and k1[0] == -1.0 and a3inv == 1.0
+    # kick ahead over half of rung 2's step (t_max / 4): int_1^{1+1/32} t^(-2/3) dt
+    assert abs(k2[2] - 3 * ((1 + t_max / 8) ** (1 / 3) - 1)) < 1e-12
+    drift, k1, k2, a3inv = oc.rung_advance(cs, t_max / 4, t_max, 2.0 / 3.0, 1.0, 0.0)
+    assert float(cs["time"]) == t_max / 4
+    assert k1[1] == 0.0 and k1[0] == -1.0  # rungs 0 and 1: time below their steps
+    t1 = 1 + t_max / 4
+    assert abs(k1[2] - 3 * (t1 ** (1 / 3) - (t1 - t_max / 8) ** (1 / 3))) < 1e-12
+    assert abs(drift - 3 * (1 - t1 ** (-1 / 3))) < 1e-12
+    assert abs(cs["a"] - t1 ** (2 / 3)) < 1e-12 and a3inv == 1.0

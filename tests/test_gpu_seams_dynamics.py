@@ -210,3 +210,71 @@ def test_cosmo_leapfrog_static_limit():
     assert abs(st[0] - 1.0) < 1e-9
     assert np.abs(x1.astype(np.int64) - x2.astype(np.int64)).max() <= 2
     assert np.abs(v1 - v2).max() <= 1e-6 * np.abs(v1).max()
+
+
+def test_cosmo_leapfrog_matches_oracle(oracle_mod):
+    """tg_leapfrog_cosmo with an evolving scale factor (a = 1 to ~1.3 over
+    three steps, H0 = 100 in code units): the FP64 path against the oracle's
+    KDK factors (its restatement of cosmos::advance_to_time) driving its
+    kick / drift and FP64 forces."""
+    import cosmo as oc
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.clustered(16, 3)
+    n = len(x)
+    H0, om, ol = 100.0, 0.3, 0.7
+    a0 = 1.0
+    st = [a0, H0, 0.0]  # da/dt = H0 at a = 1 (omega_m + omega_lambda = 1)
+    dt, steps = 1e-3, 3
+    with tg.GravitySolver(n, theta=0.7, precision="f64") as s:
+        s.set_particles(x)
+        st_lib = s.leapfrog_cosmo(dt, steps, list(st), H0=H0, omega_m=om, omega_lambda=ol)
+        xg, vg = s.get_particles()
+    o = oracle_mod.Oracle(theta=0.7).set_particles(x)
+    o.build().multipoles().walk().evaluate(fp64=True)
+    st_or = list(st)
+    for _ in range(steps):
+        st_or, f = oc.kdk_factors(st_or, dt, H0, om, ol)
+        o.kick(f[0])
+        o.drift(f[1])
+        o.build().multipoles().walk().evaluate(fp64=True)
+        o.kick(f[2])
+    xo, vo = o.particles()
+    assert list(st_lib) == list(st_or)
+    assert st_or[0] > 1.2 * a0  # the scale factor evolved
+    dxi = (xg.astype(np.int64) - xo.astype(np.int64) + 2 ** 31) % 2 ** 32 - 2 ** 31
+    assert np.abs(dxi).max() <= 64, np.abs(dxi).max()
+    assert np.abs(vg - vo).max() <= 1e-6 * np.abs(vo).max()
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_fused_kick_drift_equals_separate_calls(precision):
+    """tg_leapfrog (closing kick, opening kick and drift fused in one pass)
+    against tg_kick, tg_drift, tg_solve_gravity, tg_kick called one by one:
+    bit-identical positions and velocities."""
+    import tigergrav_b200 as tg
+    from tigergrav_b200 import ics
+    x = ics.clustered(16, 4)
+    n = len(x)
+    dt = 1e-3
+    with tg.GravitySolver(n, theta=0.7, precision=precision) as a, \
+            tg.GravitySolver(n, theta=0.7, precision=precision) as b:
+        a.set_particles(x).leapfrog(dt, 4)
+        b.set_particles(x).solve_gravity()
+        for _ in range(4):
+            b.kick(0.5 * dt)
+            b.drift(dt)
+            b.solve_gravity()
+            b.kick(0.5 * dt)
+        xa, va = a.get_particles()
+        xb, vb = b.get_particles()
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+        # the fused call alone: close + open + drift
+        a.solve_gravity()
+        b.solve_gravity()
+        a.kick_drift(0.25 * dt, 0.75 * dt, 2 * dt)
+        b.kick(0.25 * dt)
+        b.kick(0.75 * dt)
+        b.drift(2 * dt)
+        assert np.array_equal(a.get_particles()[0], b.get_particles()[0])
+        assert np.array_equal(a.get_particles()[1], b.get_particles()[1])

@@ -102,6 +102,47 @@ def test_rung_steps_match_oracle(precision):
 
 
 @pytest.mark.gpu
+def test_rung_steps_cosmo_match_oracle():
+    """Cosmological rung steps (tg_rung_step_cosmo): the expansion, kick_dt1 /
+    kick_dt2 per rung, the drift factor and the a^-3 rung choice against the
+    oracle's restatement of cosmo_advance and part_vect_kick -- positions,
+    velocities, rungs and the cosmology state bit-identical over 12 steps."""
+    import cosmo as oc
+    from tigergrav_b200 import ics
+    from tigergrav_b200.solver import GravitySolver, cosmo_rung_state
+    x = ics.halos(4096, seed=3)
+    n = len(x)
+    H0, om, ol = 2.0, 0.3, 0.7  # a grows by ~3% over t_max = 1/64
+    a0, adot0 = 1.0, 2.0
+    with GravitySolver(n, theta=0.7) as s:
+        ref, full = _stepper(x, s.params.soft_len)
+        ref.cosmo = dict(H0=H0, omega_m=om, omega_lambda=ol, state=oc.rung_state(a0, adot0))
+        s.set_particles(x)
+        cs = cosmo_rung_state(a0, adot0)
+        state = None
+        for k in range(12):
+            state = s.rung_step_cosmo(state, cs, H0, om, ol, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+            want = ref.step()
+            assert state == pytest.approx(want), k
+            xs, vs = s.get_particles()
+            assert np.array_equal(s.rungs(), ref.rung), k
+            assert np.array_equal(xs, ref.x), k
+            assert np.array_equal(vs, ref.v), k
+            c = ref.cosmo["state"]
+            assert (cs.a, cs.adot, cs.tau, cs.a_last) == (c["a"], c["adot"], c["tau"], c["a_last"]), k
+            assert np.float32(cs.time) == c["time"] and list(cs.kick1) == c["kick1"], k
+        full.close()
+        assert cs.a > 1.01 * a0
+        # the factors differ from the static ones: the same steps without cosmology end elsewhere
+        with GravitySolver(n, theta=0.7) as s0:
+            s0.set_particles(x)
+            st0 = None
+            for k in range(12):
+                st0 = s0.rung_step(st0, t_max=T_MAX, dt_max=DT_MAX, eta=ETA)
+            assert not np.array_equal(s0.get_particles()[1], ref.v)
+
+
+@pytest.mark.gpu
 def test_rung_step_forces_state():
     from tigergrav_b200 import _lib, ics
     from tigergrav_b200.solver import GravitySolver

@@ -38,6 +38,11 @@ class tg_rung_state(C.Structure):
                 ("num_active", C.c_int64), ("t", C.c_double)]
 
 
+class tg_cosmo_rung_state(C.Structure):
+    _fields_ = [("a", C.c_double), ("adot", C.c_double), ("tau", C.c_double), ("a_last", C.c_double),
+                ("time", C.c_float), ("reserved", C.c_int32), ("kick1", C.c_double * 31)]
+
+
 class tg_stats(C.Structure):
     _fields_ = [("n", C.c_int64), ("nodes", C.c_int64), ("leaves", C.c_int64), ("depth", C.c_int32),
                 ("walk_retries", C.c_int32), ("ref_stats", C.c_uint64 * 6), ("counts", C.c_uint64 * 8),
@@ -51,7 +56,7 @@ class tg_stats(C.Structure):
 EXPORTS = [
     "tg_error_string", "tg_version", "tg_create", "tg_destroy", "tg_set_particles", "tg_get_particles",
     "tg_build", "tg_multipoles", "tg_walk", "tg_set_walk_capacity", "tg_forces", "tg_solve_gravity", "tg_get_forces",
-    "tg_get_forces_f64", "tg_kick", "tg_drift", "tg_energy", "tg_leapfrog", "tg_get_stats", "tg_memory_report",
+    "tg_get_forces_f64", "tg_kick", "tg_drift", "tg_kick_drift", "tg_energy", "tg_leapfrog", "tg_get_stats", "tg_memory_report",
     "tg_num_nodes",
     "tg_get_nodes", "tg_get_perm", "tg_list_size", "tg_get_list", "tg_gravity_PP_direct",
     "tg_gravity_PP_ewald", "tg_gravity_PC_direct", "tg_gravity_PC_ewald", "tg_gravity_CC_direct",
@@ -59,7 +64,7 @@ EXPORTS = [
     "tg_energy_noalloc", "tg_forward", "tg_backward", "tg_tidal", "tg_batch_create", "tg_batch_destroy",
     "tg_batch_size", "tg_batch_set_particles", "tg_batch_autotune", "tg_batch_solve", "tg_batch_leapfrog",
     "tg_batch_get_forces", "tg_cosmo_kdk", "tg_leapfrog_cosmo", "tg_load_gadget1",
-    "tg_find_groups", "tg_set_fof_retry_limit", "tg_group_catalog", "tg_rung_step", "tg_get_rungs",
+    "tg_find_groups", "tg_set_fof_retry_limit", "tg_group_catalog", "tg_rung_step", "tg_rung_step_cosmo", "tg_cosmo_rung_init", "tg_get_rungs",
 ]
 
 
@@ -91,6 +96,7 @@ def _load():
     L.tg_get_forces_f64.argtypes = [vp, vp, vp, i32, vp]
     L.tg_kick.argtypes = [vp, d, vp]
     L.tg_drift.argtypes = [vp, d, vp]
+    L.tg_kick_drift.argtypes = [vp, d, d, d, vp]
     L.tg_energy.argtypes = [vp, vp, vp]
     L.tg_leapfrog.argtypes = [vp, d, i32, vp]
     L.tg_get_stats.argtypes = [vp, P(tg_stats)]
@@ -133,6 +139,9 @@ def _load():
     L.tg_group_catalog.argtypes = [vp, d, vp, i64, P(i64), vp]
     L.tg_rung_step.argtypes = [vp, P(tg_rung_params), P(tg_rung_state), i32, vp]
     L.tg_get_rungs.argtypes = [vp, vp, i32, vp]
+    L.tg_rung_step_cosmo.argtypes = [vp, P(tg_rung_params), P(tg_rung_state), P(tg_cosmo_params),
+                                     P(tg_cosmo_rung_state), i32, vp]
+    L.tg_cosmo_rung_init.argtypes = [P(tg_cosmo_rung_state), d, d]
     return L
 
 

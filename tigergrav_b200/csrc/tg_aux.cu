@@ -174,6 +174,59 @@ __global__ void k_drift(int64_t n, int4 *pos, const float4 *vel, float dt) {
     pos[i] = p;
 }
 
+/* The kick that closes one step, the kick that opens the next and the drift
+ * between them, in one pass over the particles (the reference fuses its kick
+ * into the force stage, src/tree.cpp:630): the same roundings as tg_kick
+ * twice and tg_drift, v = (v + float(g closeG)) + float(g openG), then
+ * x = wrap(x + v dt) requantised.  do_close = 0 skips the first kick. */
+__global__ void k_kick_drift(int64_t n, int4 *pos, float4 *vel, const float4 *acc, const double *accd, double closeG,
+                             double openG, int do_close, float dt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = vel[i];
+    double g[3];
+    if (accd) {
+        for (int d = 0; d < 3; d++) g[d] = accd[4 * i + 1 + d];
+    } else {
+        const float4 a = acc[i];
+        g[0] = a.y;
+        g[1] = a.z;
+        g[2] = a.w;
+    }
+    if (do_close) {
+        v.x = __fadd_rn(v.x, __double2float_rn(__dmul_rn(g[0], closeG)));
+        v.y = __fadd_rn(v.y, __double2float_rn(__dmul_rn(g[1], closeG)));
+        v.z = __fadd_rn(v.z, __double2float_rn(__dmul_rn(g[2], closeG)));
+    }
+    v.x = __fadd_rn(v.x, __double2float_rn(__dmul_rn(g[0], openG)));
+    v.y = __fadd_rn(v.y, __double2float_rn(__dmul_rn(g[1], openG)));
+    v.z = __fadd_rn(v.z, __double2float_rn(__dmul_rn(g[2], openG)));
+    vel[i] = v;
+    int4 p = pos[i];
+    int *pp[3] = {&p.x, &p.y, &p.z};
+    const float vv[3] = {v.x, v.y, v.z};
+    for (int d = 0; d < 3; d++) {
+        double x = __dadd_rn(pos2d(*pp[d]), (double)__fmul_rn(vv[d], dt));
+        for (int it = 0; it < 4 && x >= 1.0; it++) x = __dadd_rn(x, -1.0);
+        for (int it = 0; it < 4 && x < 0.0; it++) x = __dadd_rn(x, 1.0);
+        *pp[d] = d2pos(x);
+    }
+    pos[i] = p;
+}
+
+int kick_drift(Solver &S, double dt_close, double dt_open, double dt_drift, cudaStream_t st) {
+    if (!S.have_forces) return TG_ERR_STATE;
+    const int64_t n = S.n;
+    const bool f64 = S.prm.precision == TG_PREC_F64;
+    k_kick_drift<<<(int)((n + 255) / 256), 256, 0, st>>>(n, S.pos.p, S.vel.p, f64 ? nullptr : S.acc.p,
+                                                         f64 ? S.accd.p : nullptr, dt_close * S.prm.G,
+                                                         dt_open * S.prm.G, dt_close != 0.0 ? 1 : 0,
+                                                         (float)dt_drift);
+    TG_TRY(launched(S));
+    S.have_tree = S.have_multipoles = S.have_lists = S.have_forces = false;
+    return TG_OK;
+}
+
 int kick(Solver &S, double dt, cudaStream_t st) {
     if (!S.have_forces) return TG_ERR_STATE;
     const int64_t n = S.n;

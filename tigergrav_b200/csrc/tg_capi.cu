@@ -405,6 +405,8 @@ int tg_build(tg_solver *s, void *stream) {
     if (S.n <= 0) return TG_ERR_STATE;
     cudaStream_t st = STREAM(stream);
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[0], st));
+    S.kd_timed = S.kd_pending; /* ev[7] .. ev[0]: the fused kick-drift before this build */
+    S.kd_pending = false;
     TG_TRY(tree_build(S, st));
     if (S.have_events) TG_CUDA(cudaEventRecord(S.ev[1], st));
     return TG_OK;
@@ -504,15 +506,30 @@ int tg_energy(tg_solver *s, double out[5], void *stream) {
     return energy(s->S, out, STREAM(stream));
 }
 
+int tg_kick_drift(tg_solver *s, double dt_close, double dt_open, double dt_drift, void *stream) {
+    CHECK_HANDLE(s);
+    if (!std::isfinite(dt_close) || !std::isfinite(dt_open) || !std::isfinite(dt_drift)) return TG_ERR_ARG;
+    if (s->S.n <= 0) return TG_ERR_STATE;
+    cudaStream_t st = STREAM(stream);
+    if (s->S.have_events) TG_CUDA(cudaEventRecord(s->S.ev[7], st));
+    TG_TRY(kick_drift(s->S, dt_close, dt_open, dt_drift, st));
+    s->S.kd_pending = true;
+    return TG_OK;
+}
+
 int tg_leapfrog(tg_solver *s, double dt, int n_steps, void *stream) {
     CHECK_HANDLE(s);
     if (n_steps < 0 || !std::isfinite(dt)) return TG_ERR_ARG;
     if (!s->S.have_forces) TG_TRY(tg_solve_gravity(s, stream));
+    if (n_steps == 0) return TG_OK;
+    /* K D [solve] K per step, with each step's closing kick fused with the
+     * next step's opening kick and drift: the same arithmetic as kick, drift,
+     * solve, kick */
+    TG_TRY(tg_kick_drift(s, 0.0, 0.5 * dt, dt, stream));
     for (int k = 0; k < n_steps; k++) {
-        TG_TRY(tg_kick(s, 0.5 * dt, stream));
-        TG_TRY(tg_drift(s, dt, stream));
         TG_TRY(tg_solve_gravity(s, stream));
-        TG_TRY(tg_kick(s, 0.5 * dt, stream));
+        if (k + 1 < n_steps) TG_TRY(tg_kick_drift(s, 0.5 * dt, 0.5 * dt, dt, stream));
+        else TG_TRY(tg_kick(s, 0.5 * dt, stream));
     }
     return TG_OK;
 }
@@ -674,6 +691,8 @@ int tg_get_stats(tg_solver *s, tg_stats *out) {
         phase_ms(S, 4, 5, &S.st.ms_leaves);
         S.st.ms_pp = 0.0;
         if (S.pp_timed) phase_ms(S, 6, 5, &S.st.ms_pp);
+        S.st.ms_kick_drift = 0.0;
+        if (S.kd_timed) phase_ms(S, 7, 0, &S.st.ms_kick_drift);
     }
     S.st.launches = S.launches;
     S.st.device_bytes = (int64_t)g_dev_bytes.load();

@@ -39,14 +39,20 @@ static void cosmo_advance_to(Cosmos &c, double t0, const tg_cosmo_params &p) {
             dt = std::abs(t0 - t) * sgn;
         }
         const double a = c.a, ad = c.adot;
-        /* four stages of (tau, a, adot, drift, kick) */
-        const double k1[5] = {dt / a, ad * dt, dadot(a) * dt, dt / (a * a), dt / a};
-        const double a2 = a + 0.5 * k1[1], ad2 = ad + 0.5 * k1[2];
-        const double k2[5] = {dt / a2, ad2 * dt, dadot(a2) * dt, dt / (a2 * a2), dt / a2};
-        const double a3 = a + 0.5 * k2[1], ad3 = ad + 0.5 * k2[2];
-        const double k3[5] = {dt / a3, ad3 * dt, dadot(a3) * dt, dt / (a3 * a3), dt / a3};
-        const double a4 = a + k3[1], ad4 = ad + k3[2];
-        const double k4[5] = {dt / a4, ad4 * dt, dadot(a4) * dt, dt / (a4 * a4), dt / a4};
+        /* four stages of (tau, a, adot, drift, kick): each rate times dt, as
+         * the reference's lambdas give them ((1 / a) dt, not dt / a) */
+        auto stage = [&](double aa, double aad, double *k) {
+            k[0] = (1.0 / aa) * dt;
+            k[1] = aad * dt;
+            k[2] = dadot(aa) * dt;
+            k[3] = (1.0 / (aa * aa)) * dt;
+            k[4] = (1.0 / aa) * dt;
+        };
+        double k1[5], k2[5], k3[5], k4[5];
+        stage(a, ad, k1);
+        stage(a + 0.5 * k1[1], ad + 0.5 * k1[2], k2);
+        stage(a + 0.5 * k2[1], ad + 0.5 * k2[2], k3);
+        stage(a + k3[1], ad + k3[2], k4);
         double d[5];
         for (int q = 0; q < 5; q++) d[q] = (k1[q] + 2.0 * (k2[q] + k3[q]) + k4[q]) / 6.0;
         c.tau += d[0];
@@ -86,13 +92,15 @@ extern "C" int tg_leapfrog_cosmo(tg_solver *s, const tg_cosmo_params *p, double 
                                  void *stream) {
     if (!s || !p || !state || n_steps < 0) return TG_ERR_ARG;
     if (!s->S.have_forces) TG_TRY(tg_solve_gravity(s, stream));
+    /* each step's closing kick fused with the next step's opening kick and drift */
+    double close = 0.0;
     for (int k = 0; k < n_steps; k++) {
         double f[3];
         TG_TRY(tg_cosmo_kdk(p, state, dt, f));
-        TG_TRY(tg_kick(s, f[0], stream));
-        TG_TRY(tg_drift(s, f[1], stream));
+        TG_TRY(tg_kick_drift(s, close, f[0], f[1], stream));
         TG_TRY(tg_solve_gravity(s, stream));
-        TG_TRY(tg_kick(s, f[2], stream));
+        close = f[2];
     }
+    if (n_steps > 0) TG_TRY(tg_kick(s, close, stream));
     return TG_OK;
 }

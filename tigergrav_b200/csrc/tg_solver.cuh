@@ -152,6 +152,8 @@ struct Solver {
     cudaEvent_t ev[8];
     bool have_events = false;
     bool pp_timed = false; /* ev[6] marks the start of the FP32 PP kernel in the last solve */
+    bool kd_timed = false; /* ev[7] marks a fused kick-drift that the last solve's build followed */
+    bool kd_pending = false;
     tg_stats st{};
     int num_sms = 148;
     int64_t launches = 0; /* kernels of this library launched on this handle */
@@ -209,6 +211,7 @@ int tree_walk(Solver &S, cudaStream_t st);
 int gravity_forces(Solver &S, cudaStream_t st);
 int kick(Solver &S, double dt, cudaStream_t st);
 int drift(Solver &S, double dt, cudaStream_t st);
+int kick_drift(Solver &S, double dt_close, double dt_open, double dt_drift, cudaStream_t st);
 int energy(Solver &S, double out[5], cudaStream_t st);
 int truth(Solver &S, const int64_t *samples, int64_t ns, double alpha, double *phi, double *g, cudaStream_t st);
 int read_err(Solver &S, cudaStream_t st, uint32_t *err);

@@ -27,7 +27,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import lib, check, tg_params, tg_stats, tg_cosmo_params, tg_rung_params, tg_rung_state, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, \
+from ._lib import lib, check, tg_params, tg_stats, tg_cosmo_params, tg_rung_params, tg_rung_state, tg_cosmo_rung_state, TG_HOST, TG_DEVICE, TG_PREC_F32, TG_PREC_F64, \
     LIST_KINDS
 
 
@@ -162,6 +162,13 @@ class GravitySolver:
     def drift(self, dt, stream=None):
         check("tg_drift", lib.tg_drift(self.h, float(dt), _stream(stream)))
 
+    def kick_drift(self, dt_close, dt_open, dt_drift, stream=None):
+        """The closing kick of one step, the opening kick of the next and the
+        drift, in one pass (dt_close = 0 skips the first kick)."""
+        check("tg_kick_drift", lib.tg_kick_drift(self.h, float(dt_close), float(dt_open), float(dt_drift),
+                                                 _stream(stream)))
+        return self
+
     def leapfrog(self, dt, n_steps, stream=None):
         check("tg_leapfrog", lib.tg_leapfrog(self.h, float(dt), int(n_steps), _stream(stream)))
 
@@ -237,6 +244,20 @@ class GravitySolver:
                                                _stream(stream)))
         return dict(itime=st.itime, max_rung=st.max_rung, min_rung=st.min_rung, num_active=st.num_active, t=st.t)
 
+    def rung_step_cosmo(self, state, cstate, H0, omega_m=0.3, omega_lambda=0.7, t_max=1.0, dt_max=None, eta=0.2,
+                        all_forces=False, stream=None):
+        """rung_step with the reference's cosmological kick and drift factors.
+        cstate: a tg_cosmo_rung_state (from cosmo_rung_state()), updated in place."""
+        st = tg_rung_state(0, -1, 0, 0, 0, 0.0)
+        if state is not None:
+            st.itime, st.max_rung, st.min_rung = state["itime"], state["max_rung"], state["min_rung"]
+            st.num_active, st.t = state["num_active"], state["t"]
+        p = tg_rung_params(float(t_max), float(t_max if dt_max is None else dt_max), float(eta))
+        cp = tg_cosmo_params(float(H0), float(omega_m), float(omega_lambda))
+        check("tg_rung_step_cosmo", lib.tg_rung_step_cosmo(self.h, C.byref(p), C.byref(st), C.byref(cp),
+                                                           C.byref(cstate), int(bool(all_forces)), _stream(stream)))
+        return dict(itime=st.itime, max_rung=st.max_rung, min_rung=st.min_rung, num_active=st.num_active, t=st.t)
+
     def rungs(self, stream=None) -> np.ndarray:
         """Per-particle rungs in caller order (int8)."""
         r = np.zeros(self.n, np.int8)
@@ -264,7 +285,8 @@ class GravitySolver:
         return dict(n=s.n, nodes=s.nodes, leaves=s.leaves, depth=s.depth, walk_retries=s.walk_retries,
                     ref_stats=dict(zip(refk, map(int, s.ref_stats))), counts=dict(zip(kinds, map(int, s.counts))),
                     flops=s.flops, launches=s.launches, device_bytes=s.device_bytes, ms=dict(build=s.ms_build, multipoles=s.ms_multipoles, walk=s.ms_walk,
-                                           nodes=s.ms_nodes, leaves=s.ms_leaves, pp=s.ms_pp))
+                                           nodes=s.ms_nodes, leaves=s.ms_leaves, pp=s.ms_pp,
+                                           kick_drift=s.ms_kick_drift))
 
     def memory(self) -> dict:
         """Device bytes per buffer of this handle (and "total")."""
@@ -370,6 +392,13 @@ class GravityBatch:
         g = np.zeros((self.n, 3), np.float32)
         check("tg_batch_get_forces", lib.tg_batch_get_forces(self.h, phi.ctypes.data, g.ctypes.data, TG_HOST))
         return phi, g
+
+
+def cosmo_rung_state(a=1.0, adot=None, H0=None):
+    """A fresh cosmological rung-step state at scale factor a (adot defaults to H0)."""
+    cs = tg_cosmo_rung_state()
+    check("tg_cosmo_rung_init", lib.tg_cosmo_rung_init(C.byref(cs), float(a), float(H0 if adot is None else adot)))
+    return cs
 
 
 def cosmo_kdk(state, dt, H0, omega_m=0.3, omega_lambda=0.7):
