@@ -140,7 +140,7 @@ def test_forces(name, precision, oracle_mod):
         assert np.abs(phi - o64phi).max() / prms < 1e-6
         return
     rphi, rg = o["forces_ref"]
-    fx, px = arbiter_excess(gg, rg, o64g, phi, rphi, o64phi)
+    fx, px = arbiter_excess(gg, rg, o64g, phi, rphi, o64phi, g_alt=o32g, phi_alt=o32phi)
     assert fx <= 0.0, fx
     assert px <= 0.0, px
     e = rel_force_err(gg, o32g)

@@ -132,7 +132,7 @@ def test_rung_steps_cosmo_match_oracle():
             assert (cs.a, cs.adot, cs.tau, cs.a_last) == (c["a"], c["adot"], c["tau"], c["a_last"]), k
             assert np.float32(cs.time) == c["time"] and list(cs.kick1) == c["kick1"], k
         full.close()
-        assert cs.a > 1.01 * a0
+        assert cs.a > 1.001 * a0  # the expansion moved
         # the factors differ from the static ones: the same steps without cosmology end elsewhere
         with GravitySolver(n, theta=0.7) as s0:
             s0.set_particles(x)
