@@ -7,7 +7,7 @@ tests/test_oracle_golden.py).
   forces    FP64 path vs the oracle's FP64 evaluation: 1e-6; FP32 path: per
             particle no further from the FP64 evaluation of the same lists
             than the reference's own kernels are, plus 1e-5 of
-            max(|g|, g_rms / 4) (helpers.arbiter_excess)
+            max(|g|, g_rms / 2) (helpers.arbiter_excess)
 """
 
 import numpy as np

@@ -12,7 +12,7 @@ on, leaf 64, at the literal theta 0.7 and at theta 0.2 (RMS force error
                   the FP64 evaluation of the same lists than the reference's
                   own arithmetic is (its kernels, src/gravity.cpp via
                   oracle/_ref, or their restatement summed in another order),
-                  + 1e-5 of max(|g|, g_rms / 4) (helpers.arbiter_excess)
+                  + 1e-5 of max(|g|, g_rms / 2) (helpers.arbiter_excess)
   evolution       10 kick-drift-kick steps at dt = 1e-3 (theta 0.7) against
                   the oracle stepper driving the reference's kernels
 """
