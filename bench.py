@@ -660,7 +660,7 @@ def main():
 
 def bench_batch(args, w, cfg):
     """The batching workload: all boxes per step through tg_batch_solve (boxes
-    on 8 streams, leaf size autotuned per box over 16..128).  The batch runs on
+    on 16 streams, leaf size autotuned per box over 16..128).  The batch runs on
     its own streams from host threads, so a step is timed by the host clock
     around the call (which returns after every stream has finished)."""
     import torch
@@ -668,7 +668,7 @@ def bench_batch(args, w, cfg):
     from tigergrav_b200 import ics
     counts, x = ics.batch(w["nboxes"], w["seed"])
     n = int(counts.sum())
-    b = tg.GravityBatch(counts, theta=args.theta, precision=args.precision, nstreams=8)
+    b = tg.GravityBatch(counts, theta=args.theta, precision=args.precision, nstreams=16)
     b.set_particles(x)
     t0 = time.perf_counter()
     chosen = b.autotune((16, 32, 64, 128))
@@ -700,7 +700,7 @@ def bench_batch(args, w, cfg):
     b.close()
     mps = float(np.mean(ms))
     cfg.update({"particles_total": n, "boxes": int(len(counts)), "leaf_sizes_chosen": chosen.tolist(),
-                "autotune_s": t_tune, "streams": 8, "timing": "host clock around each batched call"})
+                "autotune_s": t_tune, "streams": 16, "timing": "host clock around each batched call"})
     line = {"metric": "Mparticles/s per batched force eval (64 boxes)", "value": n / (mps * 1e-3) / 1e6,
             "unit": "Mparticles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": mps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,

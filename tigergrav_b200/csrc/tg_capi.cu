@@ -31,6 +31,14 @@ int read_err(Solver &S, cudaStream_t st, uint32_t *err) {
     return TG_OK;
 }
 
+int read_small(Solver &S, cudaStream_t st, void *dst, const void *src, size_t bytes) {
+    if (bytes > 2048 || !S.h_small) return TG_ERR_ARG;
+    TG_CUDA(cudaMemcpyAsync(S.h_small + 2048, src, bytes, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(dst, S.h_small + 2048, bytes);
+    return TG_OK;
+}
+
 EwaldTables solver_tables(Solver &S);
 int seam_pp(Solver *, const tg_params &, int, int, int64_t, const int64_t *, const int32_t *, const int64_t *,
             const int32_t *, double *, const EwaldTables &, cudaStream_t);
@@ -285,6 +293,7 @@ int tg_create(const tg_params *params, tg_solver **out) {
     if (rc == TG_OK) rc = ensure(S.dev_cnt, 16);
     if (rc == TG_OK && cudaMallocHost(&S.h_err, sizeof(uint32_t) * 4) != cudaSuccess) rc = TG_ERR_NOMEM;
     if (rc == TG_OK && cudaMallocHost(&S.h_cnt, sizeof(unsigned long long) * 16) != cudaSuccess) rc = TG_ERR_NOMEM;
+    if (rc == TG_OK && cudaMallocHost((void **)&S.h_small, 4096) != cudaSuccess) rc = TG_ERR_NOMEM;
     if (rc == TG_OK) {
         bool ok = true;
         for (int k = 0; k < 8; k++) ok = ok && cudaEventCreate(&S.ev[k]) == cudaSuccess;
@@ -322,6 +331,10 @@ int tg_destroy(tg_solver *s) {
         release(S.nxt_pool[q]);
     }
     release(S.nx_top);
+    release(S.wk_pools);
+    release(S.wk_llen);
+    release(S.wk_loff);
+    release(S.wk_caps);
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
     release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part); release(S.ew_nt); release(S.ew_sf); release(S.ew_tpart);
@@ -333,6 +346,7 @@ int tg_destroy(tg_solver *s) {
     release(S.rung_flag); release(S.rung_scan); release(S.rung_nact); release(S.rung_out);
     if (S.h_err) cudaFreeHost(S.h_err);
     if (S.h_cnt) cudaFreeHost(S.h_cnt);
+    if (S.h_small) cudaFreeHost(S.h_small);
     if (S.h_stage) cudaFreeHost(S.h_stage);
     if (S.have_events)
         for (int k = 0; k < 8; k++) cudaEventDestroy(S.ev[k]);

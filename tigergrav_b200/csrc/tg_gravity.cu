@@ -656,8 +656,7 @@ static int node_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     TG_TRY(ensure(S.cub_tmp, stmp));
     TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, stmp, S.ew_cnt.p, S.ew_off.p, (int)(nn + 1), st));
     int32_t total = 0;
-    TG_CUDA(cudaMemcpyAsync(&total, S.ew_off.p + nn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    TG_CUDA(cudaStreamSynchronize(st));
+    TG_TRY(read_small(S, st, &total, S.ew_off.p + nn, sizeof(int32_t)));
     if (total <= 0) return TG_OK;
     TG_TRY(ensure(S.ew_part, (size_t)total * LP));
     const int g = (int)(((int64_t)total * 32 + 127) / 128);
@@ -687,8 +686,7 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     TG_TRY(ensure(S.cub_tmp, stmp));
     TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, stmp, S.ew_cnt.p, S.ew_off.p, nleaves + 1, st));
     int32_t total = 0;
-    TG_CUDA(cudaMemcpyAsync(&total, S.ew_off.p + nleaves, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    TG_CUDA(cudaStreamSynchronize(st));
+    TG_TRY(read_small(S, st, &total, S.ew_off.p + nleaves, sizeof(int32_t)));
     if (total <= 0) return TG_OK;
     TG_TRY(ensure(S.ew_part, (size_t)total * 64 * 4));
     float *tpart = nullptr;

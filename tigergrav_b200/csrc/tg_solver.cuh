@@ -99,6 +99,9 @@ struct Solver {
     DevBuf<int32_t> nxt_len[2];
     DevBuf<int32_t> nxt_pool[2];         /* two halves each: even and odd levels */
     DevBuf<unsigned long long> nx_top;   /* per level: next-list tops (direct, ewald), drain counter, spare */
+    DevBuf<int32_t *> wk_pools, wk_llen; /* device copies of the list pointer tables */
+    DevBuf<int64_t *> wk_loff;
+    DevBuf<int64_t> wk_caps;
     DevBuf<int32_t> scratch;             /* leaf drain per-warp scratch */
     int64_t scratch_per_warp = 0;
     int drain_warps = 0;
@@ -112,6 +115,10 @@ struct Solver {
     uint32_t *h_err = nullptr;          /* pinned */
     unsigned long long *h_cnt = nullptr;
     void *h_stage = nullptr;            /* pinned staging for host transfers */
+    /* pinned, 4 KB: [0, 2048) uploads of small tables, [2048, 4096) small
+     * readbacks (pageable copies would go through the driver's staging,
+     * which host threads driving other solvers contend for) */
+    unsigned char *h_small = nullptr;
     size_t h_stage_bytes = 0;
 
     /* Ewald tables */
@@ -215,6 +222,8 @@ int kick_drift(Solver &S, double dt_close, double dt_open, double dt_drift, cuda
 int energy(Solver &S, double out[5], cudaStream_t st);
 int truth(Solver &S, const int64_t *samples, int64_t ns, double alpha, double *phi, double *g, cudaStream_t st);
 int read_err(Solver &S, cudaStream_t st, uint32_t *err);
+/* bytes (<= 2048) from device memory to dst through the pinned h_small; waits for st */
+int read_small(Solver &S, cudaStream_t st, void *dst, const void *src, size_t bytes);
 int fp32_peak(int device, double *tflops, cudaStream_t st);
 
 } // namespace tg

@@ -24,6 +24,8 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <cstring>
+
 #include "tg_solver.cuh"
 
 namespace tg {
@@ -177,9 +179,12 @@ int tree_build(Solver &S, cudaStream_t st) {
         TG_TRY(ensure(S.cub_tmp, stmp));
         TG_CUDA(cub::DeviceScan::ExclusiveSum(S.cub_tmp.p, stmp, S.nd_flag.p, S.nd_scan.p, (int)count, st));
         int32_t h2[2];
-        TG_CUDA(cudaMemcpyAsync(&h2[0], S.nd_scan.p + count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        TG_CUDA(cudaMemcpyAsync(&h2[1], S.nd_flag.p + count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaMemcpyAsync(S.h_small + 2048, S.nd_scan.p + count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                st));
+        TG_CUDA(cudaMemcpyAsync(S.h_small + 2052, S.nd_flag.p + count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                st));
         TG_CUDA(cudaStreamSynchronize(st));
+        std::memcpy(h2, S.h_small + 2048, sizeof(h2));
         const int64_t nsplit = (int64_t)h2[0] + h2[1];
         S.level_leaves.push_back(count - nsplit); /* nodes of this level that stay leaves (empty ones too) */
         if (nsplit == 0) break;

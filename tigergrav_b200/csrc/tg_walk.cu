@@ -29,6 +29,7 @@
  * write out of bounds: they set a flag and the host regrows and repeats.
  */
 #include <algorithm>
+#include <cstring>
 
 #include "tg_solver.cuh"
 
@@ -424,11 +425,13 @@ int tree_walk(Solver &S, cudaStream_t st) {
     }
     TG_TRY(ensure(S.pool_top, NLIST + 2 + 2));
     TG_TRY(ensure(S.idx, nn)); /* leaf id list (idx is free after the build) */
-    /* device-side pointer tables */
+    /* device-side pointer tables, kept with the solver: a cudaFree per walk
+     * would wait for the whole device, so concurrent solvers (batches) would
+     * serialise on it */
     static_assert(NLIST == 8, "");
-    DevBuf<int32_t *> d_pools, d_llen;
-    DevBuf<int64_t *> d_loff;
-    DevBuf<int64_t> d_caps;
+    DevBuf<int32_t *> &d_pools = S.wk_pools, &d_llen = S.wk_llen;
+    DevBuf<int64_t *> &d_loff = S.wk_loff;
+    DevBuf<int64_t> &d_caps = S.wk_caps;
     TG_TRY(ensure(d_pools, NLIST));
     TG_TRY(ensure(d_llen, NLIST));
     TG_TRY(ensure(d_loff, NLIST));
@@ -442,8 +445,7 @@ int tree_walk(Solver &S, cudaStream_t st) {
         TG_TRY(launched(S));
     }
     unsigned long long nleaves_h = 0;
-    TG_CUDA(cudaMemcpyAsync(&nleaves_h, S.pool_top.p + NLIST + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    TG_CUDA(cudaStreamSynchronize(st));
+    TG_TRY(read_small(S, st, &nleaves_h, S.pool_top.p + NLIST + 2, sizeof(unsigned long long)));
     const int32_t nleaves = (int32_t)nleaves_h;
 
     /* capacities: those that served the last walk, else sized from the tree;
@@ -489,10 +491,17 @@ int tree_walk(Solver &S, cudaStream_t st) {
             h_llen[k] = S.llen[k].p;
             h_loff[k] = S.loff[k].p;
         }
-        TG_CUDA(cudaMemcpyAsync(d_pools.p, h_pools, sizeof(h_pools), cudaMemcpyHostToDevice, st));
-        TG_CUDA(cudaMemcpyAsync(d_llen.p, h_llen, sizeof(h_llen), cudaMemcpyHostToDevice, st));
-        TG_CUDA(cudaMemcpyAsync(d_loff.p, h_loff, sizeof(h_loff), cudaMemcpyHostToDevice, st));
-        TG_CUDA(cudaMemcpyAsync(d_caps.p, cap, sizeof(cap), cudaMemcpyHostToDevice, st));
+        /* the tables go up from pinned memory; the stream is waited for below
+         * (read_err) before this area is written again */
+        unsigned char *up = S.h_small;
+        std::memcpy(up, h_pools, sizeof(h_pools));
+        std::memcpy(up + 64, h_llen, sizeof(h_llen));
+        std::memcpy(up + 128, h_loff, sizeof(h_loff));
+        std::memcpy(up + 192, cap, sizeof(cap));
+        TG_CUDA(cudaMemcpyAsync(d_pools.p, up, sizeof(h_pools), cudaMemcpyHostToDevice, st));
+        TG_CUDA(cudaMemcpyAsync(d_llen.p, up + 64, sizeof(h_llen), cudaMemcpyHostToDevice, st));
+        TG_CUDA(cudaMemcpyAsync(d_loff.p, up + 128, sizeof(h_loff), cudaMemcpyHostToDevice, st));
+        TG_CUDA(cudaMemcpyAsync(d_caps.p, up + 192, sizeof(cap), cudaMemcpyHostToDevice, st));
         TG_CUDA(cudaMemsetAsync(S.pool_top.p, 0, sizeof(unsigned long long) * NLIST, st));
         /* per level: next-list tops (direct, ewald) and the drain's work counter */
         TG_CUDA(cudaMemsetAsync(S.nx_top.p, 0, sizeof(unsigned long long) * 4 * nlev, st));
@@ -533,18 +542,10 @@ int tree_walk(Solver &S, cudaStream_t st) {
         uint32_t err = 0;
         TG_TRY(read_err(S, st, &err));
         if (err & (DEV_ERR_BADINDEX | DEV_ERR_SPIN)) {
-            release(d_pools);
-            release(d_llen);
-            release(d_loff);
-            release(d_caps);
             return TG_ERR_STATE;
         }
         if (!err) break;
         if (++tries > 24) {
-            release(d_pools);
-            release(d_llen);
-            release(d_loff);
-            release(d_caps);
             return TG_ERR_CAPACITY;
         }
         /* the pool tops kept counting past a full pool: they are what this
@@ -573,10 +574,6 @@ int tree_walk(Solver &S, cudaStream_t st) {
     S.nx_cap[1] = cap_nx[1];
     S.st.walk_retries = tries;
     S.st.leaves = nleaves;
-    release(d_pools);
-    release(d_llen);
-    release(d_loff);
-    release(d_caps);
     S.have_lists = true;
     S.have_forces = false;
     return TG_OK;

@@ -339,7 +339,7 @@ class GravityBatch:
     """Many independent periodic unit boxes (counts[b] particles each, m = 1/N_b,
     soft_len = 0.02 N_b^-1/3) evaluated together on nstreams streams."""
 
-    def __init__(self, counts, theta=0.7, G=1.0, ewald=True, leaf_max=64, precision="f32", device=0, nstreams=8):
+    def __init__(self, counts, theta=0.7, G=1.0, ewald=True, leaf_max=64, precision="f32", device=0, nstreams=16):
         self.counts = np.ascontiguousarray(counts, np.int64)
         self.n = int(self.counts.sum())
         self.params = make_params(theta, 1.0, 1.0, G, ewald, leaf_max, precision, device)
