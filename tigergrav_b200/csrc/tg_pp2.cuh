@@ -4,9 +4,9 @@
  *
  * Work unit: one block of PPB_T threads per sink leaf.  A leaf of ns sinks
  * runs C = PPB_T / ns copies of them: thread t takes sink t % ns and copy
- * t / ns, copy p takes every C-th source pair starting at p, and the copies'
- * totals are added in a fixed order at the end (results do not depend on
- * scheduling).  All warps of the block share one staging area: the block
+ * t / ns, copy p takes the p-th of C contiguous shares of each stage's
+ * source pairs, and the copies' totals are added in a fixed order at the end
+ * (results do not depend on scheduling).  All warps of the block share one staging area: the block
  * stages whole source leaves (up to PPB_STAGE particles, coalesced loads of
  * each leaf's consecutive particles) and every copy of every sink reads them.
  *
@@ -25,8 +25,8 @@
  *            softened, so neither the clamp nor the spline check is needed.
  * The far form costs one packed FP32x2 addition per axis for two pairs where
  * the split form costs three; at the 256^3 clustered workload nearly all PP
- * pairs are far.  Each kind accumulates in groups of 8 source pairs (16
- * interactions) folded into Kahan-compensated totals.
+ * pairs are far.  Sums accumulate in FP32 over groups of 16 interactions
+ * (near) or 32 (far), folded into Kahan-compensated totals.
  */
 #pragma once
 
@@ -73,15 +73,15 @@ __device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, con
     a.t2 = __ffma2_rn(dz, f, a.t2);
 }
 
-/* near source pairs [q, q + n C) in steps of C with r^2 <= h^2: the
- * reference's softened kernel in place of the clamped 1/r terms */
-__device__ __noinline__ void ppb_soft_fix(const GParams &P, float h2, const SrcPair *sy, int q, int n, int C,
-                                          const SinkHL &A, PPAcc &a) {
+/* near source pairs [q, q + n) with r^2 <= h^2: the reference's softened
+ * kernel in place of the clamped 1/r terms */
+__device__ __noinline__ void ppb_soft_fix(const GParams &P, float h2, const SrcPair *sy, int q, int n, const SinkHL &A,
+                                          PPAcc &a) {
     const float hinv = rsqrtf(h2);
     const float hinv3 = hinv * hinv * hinv;
     for (int u = 0; u < n; u++) {
         float2 dx, dy, dz;
-        pp_sep2(A, sy[q + u * C], dx, dy, dz);
+        pp_sep2(A, sy[q + u], dx, dy, dz);
 #pragma unroll
         for (int e = 0; e < 2; e++) {
             const float x = e ? dx.y : dx.x, y = e ? dy.y : dy.x, z = e ? dz.y : dz.x;
@@ -99,37 +99,37 @@ __device__ __noinline__ void ppb_soft_fix(const GParams &P, float h2, const SrcP
     }
 }
 
-/* the near (split) pairs of a stage, this copy's share */
-__device__ __forceinline__ void ppb_near_stage(const GParams &P, float h2, float m, const SrcPair *sy, int phase,
-                                               int C, int np, const SinkHL &A, PPAcc &a) {
-    int q = phase;
-    for (; q + 7 * C < np; q += 8 * C) {
+/* the near (split) source pairs [q0, q1) of a stage: this copy's share */
+__device__ __forceinline__ void ppb_near_stage(const GParams &P, float h2, float m, const SrcPair *sy, int q0, int q1,
+                                               const SinkHL &A, PPAcc &a) {
+    int q = q0;
+    for (; q + 8 <= q1; q += 8) {
         float rmin = 3.0e38f;
 #pragma unroll
-        for (int u = 0; u < 8; u++) pp_pair2(A, sy[q + u * C], h2, rmin, a);
-        if (rmin <= h2) ppb_soft_fix(P, h2, sy, q, 8, C, A, a);
+        for (int u = 0; u < 8; u++) pp_pair2(A, sy[q + u], h2, rmin, a);
+        if (rmin <= h2) ppb_soft_fix(P, h2, sy, q, 8, A, a);
         a.fold(m);
     }
-    const int rest = q < np ? (np - q + C - 1) / C : 0;
-    if (rest > 0) {
+    if (q < q1) {
         float rmin = 3.0e38f;
-        for (int u = 0; u < rest; u++) pp_pair2(A, sy[q + u * C], h2, rmin, a);
-        if (rmin <= h2) ppb_soft_fix(P, h2, sy, q, rest, C, A, a);
+        for (int u = q; u < q1; u++) pp_pair2(A, sy[u], h2, rmin, a);
+        if (rmin <= h2) ppb_soft_fix(P, h2, sy, q, q1 - q, A, a);
         a.fold(m);
     }
 }
 
-/* the far pairs of a stage, this copy's share */
-__device__ __forceinline__ void ppb_far_stage(float m, const FarPair *sy, int phase, int C, int np, const float2 &ax,
+/* the far source pairs [q0, q1) of a stage: this copy's share, folded into
+ * the compensated totals every 16 source pairs (32 interactions) */
+__device__ __forceinline__ void ppb_far_stage(float m, const FarPair *sy, int q0, int q1, const float2 &ax,
                                               const float2 &ay, const float2 &az, PPAcc &a) {
-    int q = phase;
-    for (; q + 7 * C < np; q += 8 * C) {
+    int q = q0;
+    for (; q + 16 <= q1; q += 16) {
 #pragma unroll
-        for (int u = 0; u < 8; u++) ppb_far2(ax, ay, az, sy[q + u * C], a);
+        for (int u = 0; u < 16; u++) ppb_far2(ax, ay, az, sy[q + u], a);
         a.fold(m);
     }
-    if (q < np) {
-        for (; q < np; q += C) ppb_far2(ax, ay, az, sy[q], a);
+    if (q < q1) {
+        for (; q < q1; q++) ppb_far2(ax, ay, az, sy[q], a);
         a.fold(m);
     }
 }
@@ -324,13 +324,15 @@ __global__ void __launch_bounds__(PPB_T, PPB_MINB)
             const int np = (used + 1) >> 1;
             const uint32_t amax = s_amag, bmax = s_bmag;
             if (active) {
+                /* copy `phase` takes the contiguous source pairs [q0, q1) */
+                const int q0 = (np * phase) / C, q1 = (np * (phase + 1)) / C;
                 /* both forms give the int32-wrapped (nearest image) separation
                  * when every |a_i - b_j| < 2^31 */
                 const bool fits = (unsigned long long)amax + bmax < (1ull << 31);
                 if (pass == 0 && fits)
-                    ppb_near_stage(P, h2, m, stage, phase, C, np, A, a);
+                    ppb_near_stage(P, h2, m, stage, q0, q1, A, a);
                 else if (pass == 1 && fits)
-                    ppb_far_stage(m, reinterpret_cast<const FarPair *>(stage), phase, C, np, ax, ay, az, a);
+                    ppb_far_stage(m, reinterpret_cast<const FarPair *>(stage), q0, q1, ax, ay, az, a);
                 else
                     ppb_wrap_stage(P, m, m_start, m_pb, nmeta, pos, phase, C, xi, per, a);
             }
