@@ -34,7 +34,7 @@ constexpr int PPB_T = 128;     /* threads per block (one sink leaf) */
 constexpr int PPB_STAGE = 512; /* staged source particles per pass */
 constexpr int PPB_META = 64;   /* staged source leaves per pass, at most */
 #ifndef PPB_MINB
-#define PPB_MINB 8
+#define PPB_MINB 10
 #endif
 
 __device__ __forceinline__ uint32_t lanemask_lt_pp() {
