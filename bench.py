@@ -70,6 +70,10 @@ WORKLOADS = {
     "clustered128": dict(kind="clustered", nside=128, seed=2, theta_rms=0.2,
                          label="128^3 clustered P(k)~k^-2, rms displacement 0.5 spacing, seed 2"),
     "clustered64": dict(kind="clustered", nside=64, seed=5, theta_rms=0.2, label="64^3 clustered, seed 5"),
+    # a profiling case: the headline's theta and leaf size (so its near / far
+    # mix of PP source leaves) on a box whose ncu capture stays a few GB
+    "clustered96": dict(kind="clustered", nside=96, seed=2, theta_rms=0.19, leaf=48,
+                        label="96^3 clustered, seed 2 (profiling case)"),
     "uniform32": dict(kind="uniform", n=32768, seed=1, theta_rms=0.3, label="32^3 uniform, seed 1"),
     "batch64": dict(kind="batch", nboxes=64, seed=4, theta_rms=0.7,
                     label="64 boxes, N = 2^U[12,18], half uniform, half clustered"),
