@@ -335,6 +335,8 @@ int tg_destroy(tg_solver *s) {
     release(S.wk_llen);
     release(S.wk_loff);
     release(S.wk_caps);
+    release(S.wk_wx);
+    release(S.wk_kind);
     release(S.scratch); release(S.dev_err); release(S.dev_cnt);
     release(S.ew_real); release(S.ew_four); release(S.ew_Hf); release(S.ew_Hd); release(S.ew_Pf); release(S.ew_Pd);
     release(S.ew_cnt); release(S.ew_off); release(S.ew_part); release(S.ew_nt); release(S.ew_sf); release(S.ew_tpart);

@@ -102,6 +102,8 @@ struct Solver {
     DevBuf<int32_t *> wk_pools, wk_llen; /* device copies of the list pointer tables */
     DevBuf<int64_t *> wk_loff;
     DevBuf<int64_t> wk_caps;
+    DevBuf<int4> wk_wx;                  /* per node: COM and r packed for the opening tests */
+    DevBuf<int32_t> wk_kind;             /* per node: child0, or empty */
     DevBuf<int32_t> scratch;             /* leaf drain per-warp scratch */
     int64_t scratch_per_warp = 0;
     int drain_warps = 0;

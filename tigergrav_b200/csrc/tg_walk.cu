@@ -50,7 +50,24 @@ struct NodeView {
     const int32_t *pb, *pe, *child0;
     const MSrc *ms;
     const float *r, *rmax;
+    /* what the opening test reads of a check item, packed: (COM x, y, z, r
+     * bits) and child0, or NODE_EMPTY for a node without particles -- two
+     * loads per item instead of six scattered ones */
+    const int4 *wx;
+    const int32_t *kind;
 };
+
+constexpr int32_t NODE_EMPTY = -2;
+
+/* the packed records of NodeView::wx / kind, one thread per node */
+__global__ void k_walk_records(int64_t nn, const int32_t *__restrict__ pb, const int32_t *__restrict__ pe,
+                               const int32_t *__restrict__ child0, const MSrc *__restrict__ ms,
+                               const float *__restrict__ r, int4 *__restrict__ wx, int32_t *__restrict__ kind) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    wx[i] = make_int4(ms[i].x[0], ms[i].x[1], ms[i].x[2], __float_as_int(r[i]));
+    kind[i] = pe[i] == pb[i] ? NODE_EMPTY : child0[i];
+}
 
 __device__ __forceinline__ double near_sep(const double *x) {
     double d = 0.0;
@@ -107,13 +124,14 @@ __device__ __forceinline__ int classify(const WalkParams &W, const NodeView &V, 
         atomicOr(err, DEV_ERR_BADINDEX);
         return C_SKIP;
     }
-    if (V.pe[c] == V.pb[c]) return C_SKIP;
-    const MSrc &s = V.ms[c];
-    const int32_t cx[3] = {s.x[0], s.x[1], s.x[2]};
-    const float cr = V.r[c];
+    const int32_t k = V.kind[c];
+    if (k == NODE_EMPTY) return C_SKIP;
+    const int4 q = V.wx[c];
+    const int32_t cx[3] = {q.x, q.y, q.z};
+    const float cr = __int_as_float(q.w);
     const bool far = ewald_list ? far_ewald(W, X, r, rmax, cx, cr) : far_direct(W, X, r, cx, cr);
     if (far) return (item & OPENED) ? C_FAR_OPEN : C_FAR;
-    return V.child0[c] < 0 ? C_NEAR_LEAF : C_NEAR_INT;
+    return k < 0 ? C_NEAR_LEAF : C_NEAR_INT;
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -188,7 +206,7 @@ __device__ void node_stage_list(const WalkParams &W, const NodeView &V, bool ewa
         if (code == C_FAR) pool_cc[b_cc + r_cc + __popc(m_cc & lt)] = id;
         if (code == C_NEAR_LEAF) pool_nx[b_nx + r_lf + __popc(m_lf & lt)] = (int32_t)(item | OPENED);
         if (code == C_NEAR_INT) {
-            const int32_t c0 = V.child0[id];
+            const int32_t c0 = V.kind[id]; /* an internal node: its child0 */
             const int64_t q = b_nx + n_lf + 2 * (r_int + __popc(m_in & lt));
             pool_nx[q] = c0;
             pool_nx[q + 1] = c0 + 1;
@@ -311,7 +329,7 @@ __device__ void drain_list(const WalkParams &W, const NodeView &V, bool ewald_li
             if (pc) outPC[n_pc + __popc(m_pc & lt)] = id;
             if (lf) nxt[r_lf + __popc(m_lf & lt)] = (int32_t)(item | OPENED);
             if (in_) {
-                const int32_t c0 = V.child0[id];
+                const int32_t c0 = V.kind[id]; /* an internal node: its child0 */
                 const int32_t q = n_lf + 2 * (r_int + __popc(m_in & lt));
                 nxt[q] = c0;
                 nxt[q + 1] = c0 + 1;
@@ -413,7 +431,12 @@ int tree_walk(Solver &S, cudaStream_t st) {
     W.r_ewald = (float)(2.0 * S.prm.theta * std::pow(1.0e-3 / 8.0, 1.0 / 3.0));
     W.ewald = S.prm.ewald ? 1 : 0;
     W.nact = S.walk_nact;
-    NodeView V{S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p, S.nd_r.p, S.nd_rmax.p};
+    TG_TRY(ensure(S.wk_wx, nn));
+    TG_TRY(ensure(S.wk_kind, nn));
+    k_walk_records<<<(int)((nn + 255) / 256), 256, 0, st>>>(nn, S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p,
+                                                            S.nd_r.p, S.wk_wx.p, S.wk_kind.p);
+    TG_TRY(launched(S));
+    NodeView V{S.nd_pb.p, S.nd_pe.p, S.nd_child0.p, S.nd_ms.p, S.nd_r.p, S.nd_rmax.p, S.wk_wx.p, S.wk_kind.p};
 
     for (int k = 0; k < NLIST; k++) {
         TG_TRY(ensure(S.loff[k], nn));
