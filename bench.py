@@ -72,8 +72,8 @@ WORKLOADS = {
     "clustered64": dict(kind="clustered", nside=64, seed=5, theta_rms=0.2, label="64^3 clustered, seed 5"),
     # a profiling case: the headline's theta and leaf size (so its near / far
     # mix of PP source leaves) on a box whose ncu capture stays a few GB
-    "clustered96": dict(kind="clustered", nside=96, seed=2, theta_rms=0.19, leaf=48,
-                        label="96^3 clustered, seed 2 (profiling case)"),
+    "clustered72": dict(kind="clustered", nside=72, seed=2, theta_rms=0.19, leaf=48,
+                        label="72^3 clustered, seed 2 (profiling case)"),
     "uniform32": dict(kind="uniform", n=32768, seed=1, theta_rms=0.3, label="32^3 uniform, seed 1"),
     "batch64": dict(kind="batch", nboxes=64, seed=4, theta_rms=0.7,
                     label="64 boxes, N = 2^U[12,18], half uniform, half clustered"),
@@ -105,11 +105,13 @@ PP_FLOPS = 18
 # PP_E pair (cut r < 2, origin separate): 32.5 images x 44 + 30 = 1.46k.
 NODE_FLOPS = {"CC_D": 1025, "CP_D": 455, "CC_E": 13100, "CP_E": 12300}
 LEAF_FLOPS = {"PC_D": 581, "PC_E": 7800, "PP_E": 1460}
-# DRAM bytes per interaction of each kernel group, from an ncu capture of the
-# kernels on the 64^3 clustered box at theta 0.2 (dram__bytes_read.sum +
-# dram__bytes_write.sum over the capture's interactions); scaled by this
-# run's counts on the assumption that traffic grows with the interactions.
-TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 6.3, "CP_E": 6.3}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
+# DRAM bytes per interaction of each kernel group, from ncu captures
+# (dram__bytes_read.sum + dram__bytes_write.sum over the capture's
+# interactions): k_pp_leaf and k_node_ewald on the 72^3 clustered box at
+# theta 0.19, leaf 48 (the clustered72 workload); k_ewald_chunk on the 128^3
+# clustered box at theta 0.3.  Scaled by this run's counts on the assumption
+# that traffic grows with the interactions.
+TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 2.65, "CP_E": 2.65}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per interaction of a small capture, "
                   "scaled by this run's interaction counts")
 
