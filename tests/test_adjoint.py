@@ -88,20 +88,33 @@ def test_adjoint_matches_central_fd(precision):
     rng = np.random.default_rng(7)
     idx = rng.choice(n, 32, replace=False)
     dims = rng.integers(0, 3, 32)
-    errs, skipped = [], 0
-    for i, d in zip(idx, dims):
-        xp, xm = x0.copy(), x0.copy()
-        xp[i, d] = ics.double_to_pos(np.array([xd0[i, d] + h]))[0]
-        xm[i, d] = ics.double_to_pos(np.array([xd0[i, d] - h]))[0]
-        hh = ((_p2d(xp[i, d]) - _p2d(xm[i, d]) + 0.5) % 1.0) - 0.5
-        (lp, sp), (lm, sm) = loss(xp), loss(xm)
-        if sp != sm:
-            skipped += 1
-            continue
-        fd = (lp - lm) / hh
-        errs.append(abs(gx0[i, d] - fd) / abs(fd))
-    fds.close()
-    errs = np.array(errs)
+
+    def central(hstep, samples):
+        errs, nonid, skipped = [], [], 0
+        for i, d in samples:
+            xp, xm = x0.copy(), x0.copy()
+            xp[i, d] = ics.double_to_pos(np.array([xd0[i, d] + hstep]))[0]
+            xm[i, d] = ics.double_to_pos(np.array([xd0[i, d] - hstep]))[0]
+            hh = ((_p2d(xp[i, d]) - _p2d(xm[i, d]) + 0.5) % 1.0) - 0.5
+            (lp, sp), (lm, sm) = loss(xp), loss(xm)
+            if sp != sm:
+                skipped += 1
+                continue
+            fd = (lp - lm) / hh
+            errs.append(abs(gx0[i, d] - fd) / abs(fd))
+            nonid.append(abs((gx0[i, d] - w[i, d]) - (fd - w[i, d])) / abs(fd - w[i, d]))
+        return np.array(errs), np.array(nonid), skipped
+
+    errs, _, skipped = central(h, list(zip(idx, dims)))
     assert skipped <= 8
     assert np.median(errs) <= 1e-4, np.median(errs)
     assert np.percentile(errs, 90) <= 1e-3, np.percentile(errs, 90)
+    # The force term alone: dL/dx0 - w is ~2e-4 |w|, the size of the
+    # fixed-point requantisation noise of the difference at h = 1e-4 (every
+    # drift rounds to 2^-32); at h = 1e-3 that noise is 10x smaller and the
+    # non-identity part is judged on its own (measured median 6% here, 2% at
+    # 16^3, where the tree approximation of J and the noise are both smaller).
+    _, nonid, skipped = central(1e-3, list(zip(idx, dims))[:16])
+    fds.close()
+    assert skipped <= 6
+    assert np.median(nonid) <= 0.15, np.median(nonid)

@@ -110,7 +110,26 @@ template <> __device__ __forceinline__ float wrap_sep_t<float>(int32_t X, int32_
 template <> __device__ __forceinline__ double wrap_sep_t<double>(int32_t X, int32_t Y) { return wrap_sep_d(X, Y); }
 
 /* ---- per-type math ---- */
-__device__ __forceinline__ float t_rsqrt(float x) { return rsqrtf(x); }
+/* The hardware approximations of PTX (rsqrt / rcp / ex2 .approx) in their
+ * .ftz form: subnormal inputs and results flush to zero, which spares the
+ * scaling that the IEEE-subnormal forms need; every input here is a normal
+ * number (r^2 >= h^2 or >= 1e-12, 1 + 0.33 x >= 1, exponents >= -26). */
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float t_rsqrt(float x) { return rsqrt_ftz(x); }
 __device__ __forceinline__ double t_rsqrt(double x) { return 1.0 / sqrt(x); }
 __device__ __forceinline__ float t_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double t_sqrt(double x) { return sqrt(x); }
@@ -121,8 +140,8 @@ __device__ __forceinline__ double t_rcp(double x) { return 1.0 / x; }
  * approximation that the reference uses (tigergrav/simd.hpp:676-692), with
  * expf; FP64: the double-precision erfc and exp. */
 __device__ __forceinline__ float t_erfcexp(float x, float *e) {
-    const float t1 = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
-    *e = __expf(-x * x);
+    const float t1 = rcp_ftz(fmaf(0.3275911f, x, 1.0f));
+    *e = ex2_ftz(x * x * -1.4426950408889634f); /* e^-x^2 = 2^(-x^2 log2 e) */
     const float poly = t1 * (0.254829592f + t1 * (-0.284496736f + t1 * (1.421413741f + t1 * (-1.453152027f + t1 * 1.061405429f))));
     return poly * *e;
 }
@@ -372,7 +391,7 @@ __device__ __forceinline__ void ewald_origin_add(float *D, EwaldMom<float> &m, c
         }
     } else {
         ewald_image_factors<float>(r2, c[0], c[1], c[2], c[3], c[4]);
-        const float rinv = rsqrtf(r2), r2inv = rinv * rinv;
+        const float rinv = rsqrt_ftz(r2), r2inv = rinv * rinv;
         float dd = -rinv; /* direct: -1/r and its (1/r d/dr)^k: 1/r^3, -3/r^5, 15/r^7, -105/r^9 */
         c[0] -= dd;
         dd = rinv * r2inv;

@@ -41,10 +41,13 @@ template <class T, bool SEP>
 __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves,
                                                     const int32_t *__restrict__ off, const int32_t *__restrict__ pb,
                                                     const int32_t *__restrict__ pe, const MSrc *__restrict__ ms,
-                                                    const int4 *__restrict__ pos, ListView LV, EwaldTables E,
-                                                    double *__restrict__ part, const float2 *__restrict__ nt,
-                                                    const float2 *__restrict__ sf, float *__restrict__ tpart) {
+                                                    const int4 *__restrict__ pos, const int32_t *__restrict__ aabb,
+                                                    ListView LV, EwaldTables E, double *__restrict__ part,
+                                                    const float2 *__restrict__ nt, const float2 *__restrict__ sf,
+                                                    float *__restrict__ tpart) {
     __shared__ int4 sy[64];
+    __shared__ float4 s_img[SEP ? EW_IMG_CAP : 1]; /* FP32: the block's image list per source */
+    __shared__ int s_tmp[3];
     const int tid = threadIdx.x;
     const int64_t c = blockIdx.x;
     int32_t lo = 0, hi = nleaves - 1; /* the leaf: largest li with off[li] <= c */
@@ -71,6 +74,12 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
         for (int32_t e = k * EW_KPP; e < e1; e++) {
             const int32_t src = lst[e];
             const int32_t sb = pb[src], sn = pe[src] - sb;
+            EwPairing Q;
+            int nimg = 0, s0 = 0;
+            if constexpr (SEP) {
+                ew_pairing(aabb + 6 * leaf, aabb + 6 * leaf + 3, aabb + 6 * src, aabb + 6 * src + 3, 2.0f, Q);
+                nimg = ew_image_set(Q.c, Q.rr, s_img, s_tmp, s0);
+            }
             for (int32_t base = 0; base < sn; base += 64) {
                 const int32_t nsy = min(64, sn - base);
                 __syncthreads();
@@ -80,8 +89,17 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
                     const int4 y = sy[q];
                     T dX[3] = {wrap_sep_t<T>(xi[0], y.x), wrap_sep_t<T>(xi[1], y.y), wrap_sep_t<T>(xi[2], y.z)};
                     T ph, g[3];
-                    if constexpr (SEP) pp_ewald_pair_sep(E, dX, ph, g);
-                    else pp_ewald_pair<T>(E, dX, ph, g);
+                    if constexpr (SEP) {
+                        ImgList L{s_img, nimg, s0, Q.wrap, 0.0f, 0.0f, 0.0f};
+                        if (Q.wrap) { /* block-uniform */
+                            L.k0 = ew_wrap_k(Q.C[0], xi[0], Q.a[0], y.x, Q.b[0]);
+                            L.k1 = ew_wrap_k(Q.C[1], xi[1], Q.a[1], y.y, Q.b[1]);
+                            L.k2 = ew_wrap_k(Q.C[2], xi[2], Q.a[2], y.z, Q.b[2]);
+                        }
+                        pp_ewald_pair_sep(E, dX, ph, g, L);
+                    } else {
+                        pp_ewald_pair<T>(E, dX, ph, g);
+                    }
                     aphi.add(m * ph);
                     for (int d = 0; d < 3; d++) ag[d].add(m * g[d]);
                 }
@@ -98,8 +116,21 @@ __global__ void __launch_bounds__(64, EW_MINB) k_ewald_chunk(GParams P, const in
             for (int d = 0; d < 3; d++) dX[d] = sep<T>(xi[d], s.x[d], true);
 #pragma unroll
             for (int q = 0; q < MP; q++) M[q] = T(s.m[q]);
-            if constexpr (SEP) green_ewald_sep(E, dX, D);
-            else green_ewald_full<T>(E, dX, D);
+            if constexpr (SEP) {
+                EwPairing Q;
+                ew_pairing(aabb + 6 * leaf, aabb + 6 * leaf + 3, s.x, s.x, 2.1f, Q);
+                int s0;
+                const int nimg = ew_image_set(Q.c, Q.rr, s_img, s_tmp, s0);
+                ImgList L{s_img, nimg, s0, Q.wrap, 0.0f, 0.0f, 0.0f};
+                if (Q.wrap) { /* block-uniform */
+                    L.k0 = ew_wrap_k(Q.C[0], xi[0], Q.a[0], s.x[0], Q.b[0]);
+                    L.k1 = ew_wrap_k(Q.C[1], xi[1], Q.a[1], s.x[1], Q.b[1]);
+                    L.k2 = ew_wrap_k(Q.C[2], xi[2], Q.a[2], s.x[2], Q.b[2]);
+                }
+                green_ewald_sep(E, dX, D, L);
+            } else {
+                green_ewald_full<T>(E, dX, D);
+            }
             T ph, g[3];
             contract_M2P<T>(ph, g, M, D);
             aphi.add(ph);

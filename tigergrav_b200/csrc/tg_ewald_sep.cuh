@@ -109,8 +109,142 @@ __device__ __forceinline__ void pp_ewald_recip(const EwaldTables &E, const float
     }
 }
 
+/*
+ * Real-space images in lockstep.  The sinks of one leaf and the particles of
+ * one source leaf (or one source node's centre) lie within a few leaf widths
+ * of each other, so the lattice vectors that any of their pairs needs are
+ * those within R + rho of the separation of the two boxes' centres (rho: the
+ * largest deviation of a pair's separation from it).  A block lists that set
+ * once per source in lexicographic order (ew_image_set), and every thread
+ * then runs the same counted loop over it, testing its own pair's cut
+ * |X - n|^2 < R^2 per image: the lanes of a warp stay together, where the
+ * per-thread walk of ewald_images ran a different number of images per lane
+ * and spent square roots and conversions on its ranges.  The images visited,
+ * their order and their arithmetic (d = X - n in FP32) are those of
+ * ewald_images.  A pair whose nearest image wraps differently from the
+ * centres' (the centres' separation near +-1/2) shifts the list by its wrap k:
+ * n = m - k.  The |n|^2 <= 17 limit of the reference's lattice never binds in
+ * FP32: |n| <= |X| + R < sqrt(3)/2 + 2.1, so |n|^2 <= 8.
+ */
+constexpr int EW_IMG_CAP = 512; /* >= the lattice points within 3.84 + sqrt(3)/2 of any centre (436) */
+
+/* all 64 threads of the block: the lattice vectors m with |c - m| < rr in
+ * lexicographic order into img, and their count.  rr < 3.84 (two boxes of at
+ * most unit width: rho <= sqrt(3)), so at most 9 x 9 columns (nx, ny). */
+__device__ __forceinline__ int ew_image_set(const float *c, float rr, float4 *img, int *s_tmp, int &s0) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int x0 = (int)floorf(c[0] - rr), y0 = (int)floorf(c[1] - rr);
+    const int nyr = (int)floorf(c[1] + rr) - y0 + 1;
+    const int ncol = ((int)floorf(c[0] + rr) - x0 + 1) * nyr;
+    int total = 0;
+    for (int c0 = 0; c0 < ncol; c0 += 64) { /* block-uniform; column order = lexicographic (nx, ny) */
+        const int col = c0 + tid;
+        int ix = 0, iy = 0, z0 = 0, cnt = 0;
+        if (col < ncol) {
+            ix = x0 + col / nyr;
+            iy = y0 + col % nyr;
+            const float dx = c[0] - (float)ix, dy = c[1] - (float)iy;
+            const float rz2 = rr * rr - dx * dx - dy * dy;
+            if (rz2 > 0.0f) {
+                const float rz = sqrtf(rz2);
+                z0 = (int)ceilf(c[2] - rz);
+                cnt = max(0, (int)floorf(c[2] + rz) - z0 + 1);
+            }
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_tmp[w] = incl;
+        __syncthreads();
+        const int base = total + (w ? s_tmp[0] : 0) + incl - cnt;
+        for (int q = 0; q < cnt; q++)
+            if (base + q < EW_IMG_CAP) img[base + q] = make_float4((float)ix, (float)iy, (float)(z0 + q), 0.0f);
+        if (ix == 0 && iy == 0 && z0 <= 0 && 0 < z0 + cnt) s_tmp[2] = base - z0; /* m = 0: always listed */
+        total += s_tmp[0] + s_tmp[1];
+        __syncthreads();
+    }
+    s0 = s_tmp[2];
+    return min(total, EW_IMG_CAP);
+}
+
+/* the geometry of one (sink box, source) pairing for ew_image_set: centre
+ * separation c (box units), the radius rr of the set for a cut R, and whether
+ * any pair can wrap differently from the centres.  Boxes: fixed-point
+ * min / max per axis (a source point has min = max). */
+struct EwPairing {
+    int32_t a[3], b[3]; /* the sink box's and the source's centres, fixed point */
+    int32_t C[3];       /* a - b wrapped */
+    float c[3];
+    float rr;
+    bool wrap;
+};
+__device__ __forceinline__ void ew_pairing(const int32_t *sink_lo, const int32_t *sink_hi, const int32_t *src_lo,
+                                           const int32_t *src_hi, float R, EwPairing &Q) {
+    float e2 = 0.0f;
+    Q.wrap = false;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        Q.a[d] = (int32_t)(((long long)sink_lo[d] + sink_hi[d]) >> 1);
+        Q.b[d] = (int32_t)(((long long)src_lo[d] + src_hi[d]) >> 1);
+        Q.C[d] = (int32_t)((uint32_t)Q.a[d] - (uint32_t)Q.b[d]);
+        Q.c[d] = (float)Q.C[d] * 2.3283064365386963e-10f;
+        /* |x - a| + |y - b| <= ext over the two boxes, fixed point */
+        const long long ext = (((long long)sink_hi[d] - sink_lo[d]) >> 1) + (((long long)src_hi[d] - src_lo[d]) >> 1) + 2;
+        const float ef = (float)ext * 2.3283064365386963e-10f;
+        e2 += ef * ef;
+        const long long Cabs = Q.C[d] < 0 ? -(long long)Q.C[d] : (long long)Q.C[d];
+        if (Cabs + ext >= (1LL << 31)) Q.wrap = true;
+    }
+    Q.rr = R + sqrtf(e2) * 1.001f + 1.0e-3f;
+}
+/* a pair's wrap k (n = m - k) on one axis: x - y as the centres see it minus
+ * its minimum image, in units of the box */
+__device__ __forceinline__ float ew_wrap_k(int32_t C, int32_t x, int32_t ca, int32_t y, int32_t cb) {
+    const long long D = (long long)C + ((long long)x - ca) - ((long long)y - cb);
+    const long long dxi = (long long)(int32_t)((uint32_t)x - (uint32_t)y);
+    return (float)((D - dxi) >> 32);
+}
+
+/* image visitors for the Ewald sums below: the per-thread walk, or a shared list */
+struct ImgWalk {
+    template <class F> __device__ __forceinline__ void operator()(const float *X, F &&fn, float R2) const {
+        ewald_images<float>(X, fn, R2);
+    }
+};
+struct ImgList {
+    const float4 *img;
+    int n, s0;  /* s0: the index of m = 0 */
+    bool wrap;  /* block-uniform: some pair of the pairing wraps differently from the centres */
+    float k0, k1, k2;
+    template <class F> __device__ __forceinline__ void operator()(const float *X, F &&fn, float R2) const {
+        if (!wrap) { /* k = 0 for every pair: n = m, the origin at s0 for all lanes */
+            for (int s = 0; s < n; s++) {
+                const float4 m = img[s];
+                const float d[3] = {X[0] - m.x, X[1] - m.y, X[2] - m.z};
+                const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                if (s == s0) fn(d, r2, true); /* |X| < R: the origin is always inside the cut */
+                else if (r2 < R2) fn(d, r2, false);
+            }
+            return;
+        }
+        for (int s = 0; s < n; s++) {
+            const float4 m = img[s];
+            const float n0 = m.x - k0, n1 = m.y - k1, n2 = m.z - k2;
+            const float d[3] = {X[0] - n0, X[1] - n1, X[2] - n2};
+            const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (!(r2 < R2)) continue;
+            fn(d, r2, n0 == 0.0f && n1 == 0.0f && n2 == 0.0f);
+        }
+    }
+};
+
 /* PP_E pair without its reciprocal terms (those come from the leaf sums) */
-__device__ __forceinline__ void pp_ewald_pair_sep(const EwaldTables &E, const float *dX0, float &phi, float *g) {
+template <class V = ImgWalk>
+__device__ __forceinline__ void pp_ewald_pair_sep(const EwaldTables &E, const float *dX0, float &phi, float *g,
+                                                  const V &images = V()) {
     const float r2 = dX0[0] * dX0[0] + dX0[1] * dX0[1] + dX0[2] * dX0[2];
     if (!(r2 > 1.0e-12f)) { /* phi0 alone: take back what the leaf sums add for this pair */
         float ph, gr[3];
@@ -120,7 +254,7 @@ __device__ __forceinline__ void pp_ewald_pair_sep(const EwaldTables &E, const fl
         return;
     }
     float ph = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
-    ewald_images<float>(dX0, [&](const float *d, float rr2, bool origin) {
+    images(dX0, [&](const float *d, float rr2, bool origin) {
         if (origin) return;
         const float rinv = t_rsqrt(rr2);
         const float r = rr2 * rinv;
@@ -144,7 +278,8 @@ __device__ __forceinline__ void pp_ewald_pair_sep(const EwaldTables &E, const fl
 }
 
 /* green_ewald without its reciprocal terms (FP32) */
-__device__ __forceinline__ void green_ewald_sep(const EwaldTables &E, const float *X, float *D) {
+template <class V = ImgWalk>
+__device__ __forceinline__ void green_ewald_sep(const EwaldTables &E, const float *X, float *D, const V &images = V()) {
 #pragma unroll
     for (int k = 0; k < LP; k++) D[k] = 0.0f;
     const float r2 = X[0] * X[0] + X[1] * X[1] + X[2] * X[2];
@@ -157,10 +292,10 @@ __device__ __forceinline__ void green_ewald_sep(const EwaldTables &E, const floa
     }
     EwaldMom<float> mom;
     mom.init();
-    ewald_images<float>(X, [&](const float *d, float rr2, bool origin) {
+    images(X, [&](const float *d, float rr2, bool origin) {
         if (origin) ewald_origin_add(D, mom, d, rr2);
         else ewald_real_image<float>(D, mom, d, rr2);
-    });
+    }, ewald_rcut2<float>());
     ewald_mom_finish<float>(D, mom);
     D[E0()] += 0.78539816339744831f; /* pi/4 (tigergrav/green.hpp:270) */
 }

@@ -692,8 +692,8 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
     float *tpart = nullptr;
     if (f64) {
         k_ewald_chunk<double, false><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
-                                                           S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, nullptr, nullptr,
-                                                           nullptr);
+                                                           S.nd_ms.p, S.pos.p, S.nd_aabb.p, LV, E, S.ew_part.p, nullptr,
+                                                           nullptr, nullptr);
     } else {
         /* reciprocal terms per sink leaf: (cos, sin) tables per node, sums per leaf */
         const int64_t nn = S.nnodes;
@@ -705,8 +705,8 @@ static int leaf_ewald(Solver &S, const GParams &P, const ListView &LV, const Ewa
                                                                 S.pos.p, E, S.ew_nt.p, S.ew_sf.p);
         TG_TRY(launched(S));
         k_ewald_chunk<float, true><<<total, 64, 0, st>>>(P, S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p,
-                                                         S.nd_ms.p, S.pos.p, LV, E, S.ew_part.p, S.ew_nt.p, S.ew_sf.p,
-                                                         tpart);
+                                                         S.nd_ms.p, S.pos.p, S.nd_aabb.p, LV, E, S.ew_part.p, S.ew_nt.p,
+                                                         S.ew_sf.p, tpart);
     }
     TG_TRY(launched(S));
     k_ewald_reduce<<<nleaves, 64, 0, st>>>(S.idx.p, nleaves, S.ew_off.p, S.nd_pb.p, S.nd_pe.p, S.ew_part.p, S.accd.p,

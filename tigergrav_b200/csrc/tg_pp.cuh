@@ -60,7 +60,7 @@ __device__ __forceinline__ void pp_pair2(const SinkHL &A, const SrcPair &s, floa
     pp_sep2(A, s, dx, dy, dz);
     const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
     rmin = fminf(rmin, fminf(r2.x, r2.y));
-    const float2 rinv = make_float2(rsqrtf(fmaxf(r2.x, h2)), rsqrtf(fmaxf(r2.y, h2)));
+    const float2 rinv = make_float2(rsqrt_ftz(fmaxf(r2.x, h2)), rsqrt_ftz(fmaxf(r2.y, h2)));
     const float2 f = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
     a.tp = __fadd2_rn(a.tp, rinv);
     a.t0 = __ffma2_rn(dx, f, a.t0);

@@ -65,7 +65,7 @@ __device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, con
                                          PPAcc &a) {
     const float2 dx = __fadd2_rn(ax, s.x), dy = __fadd2_rn(ay, s.y), dz = __fadd2_rn(az, s.z);
     const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-    const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
     const float2 f = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
     a.tp = __fadd2_rn(a.tp, rinv);
     a.t0 = __ffma2_rn(dx, f, a.t0);
@@ -77,7 +77,7 @@ __device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, con
  * kernel in place of the clamped 1/r terms */
 __device__ __noinline__ void ppb_soft_fix(const GParams &P, float h2, const SrcPair *sy, int q, int n, const SinkHL &A,
                                           PPAcc &a) {
-    const float hinv = rsqrtf(h2);
+    const float hinv = rsqrt_ftz(h2);
     const float hinv3 = hinv * hinv * hinv;
     for (int u = 0; u < n; u++) {
         float2 dx, dy, dz;
@@ -278,36 +278,31 @@ __global__ void __launch_bounds__(PPB_T, PPB_MINB)
             __syncthreads();
             const int used = s_used, nmeta = s_nmeta;
             if (used == 0) break; /* the list is exhausted for this kind */
-            /* every thread copies particles: consecutive q are consecutive
-             * particles of one source leaf (coalesced loads) */
+            /* warp w copies the source leaves w, w + 4, ...: its lanes take
+             * consecutive particles of one leaf (coalesced loads) */
             uint32_t bmag = 0;
-            for (int q = t; q < used; q += PPB_T) {
-                int lo = 0, hi = nmeta - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (m_start[mid] <= q) lo = mid;
-                    else hi = mid - 1;
+            for (int k = t >> 5; k < nmeta; k += PPB_T / 32)
+                for (int q = m_start[k] + lane; q < m_start[k + 1]; q += 32) {
+                    const int4 y = pos[m_pb[k] + (q - m_start[k])];
+                    const int32_t o0 = rel_off(y.x, Xr[0], per, bmag);
+                    const int32_t o1 = rel_off(y.y, Xr[1], per, bmag);
+                    const int32_t o2 = rel_off(y.z, Xr[2], per, bmag);
+                    if (pass == 0) {
+                        float *e = sf + (q >> 1) * 12 + (q & 1); /* SrcPair: hx.x hx.y hy.x ... lz.y */
+                        float h, l;
+                        split_hl(o0, h, l);
+                        e[0] = -h, e[6] = -l;
+                        split_hl(o1, h, l);
+                        e[2] = -h, e[8] = -l;
+                        split_hl(o2, h, l);
+                        e[4] = -h, e[10] = -l;
+                    } else {
+                        float *e = sf + (q >> 1) * 6 + (q & 1); /* FarPair: x.x x.y y.x y.y z.x z.y */
+                        e[0] = -__int2float_rn(o0) * 2.3283064365386963e-10f;
+                        e[2] = -__int2float_rn(o1) * 2.3283064365386963e-10f;
+                        e[4] = -__int2float_rn(o2) * 2.3283064365386963e-10f;
+                    }
                 }
-                const int4 y = pos[m_pb[lo] + (q - m_start[lo])];
-                const int32_t o0 = rel_off(y.x, Xr[0], per, bmag);
-                const int32_t o1 = rel_off(y.y, Xr[1], per, bmag);
-                const int32_t o2 = rel_off(y.z, Xr[2], per, bmag);
-                if (pass == 0) {
-                    float *e = sf + (q >> 1) * 12 + (q & 1); /* SrcPair: hx.x hx.y hy.x ... lz.y */
-                    float h, l;
-                    split_hl(o0, h, l);
-                    e[0] = -h, e[6] = -l;
-                    split_hl(o1, h, l);
-                    e[2] = -h, e[8] = -l;
-                    split_hl(o2, h, l);
-                    e[4] = -h, e[10] = -l;
-                } else {
-                    float *e = sf + (q >> 1) * 6 + (q & 1); /* FarPair: x.x x.y y.x y.y z.x z.y */
-                    e[0] = -__int2float_rn(o0) * 2.3283064365386963e-10f;
-                    e[2] = -__int2float_rn(o1) * 2.3283064365386963e-10f;
-                    e[4] = -__int2float_rn(o2) * 2.3283064365386963e-10f;
-                }
-            }
             if ((used & 1) && t == 0) { /* pad: a source at 1e30 gives exactly zero terms */
                 if (pass == 0) {
                     float *e = sf + (used >> 1) * 12 + 1;
