@@ -24,7 +24,7 @@
  *            the reference's conversion gives 0.5 ulp), and no pair is
  *            softened, so neither the clamp nor the spline check is needed.
  * The far form costs one packed FP32x2 addition per axis for two pairs where
- * the split form costs three; at the 256^3 clustered workload nearly all PP
+ * the split form costs three, and reads four sources per 16-byte load; at the 256^3 clustered workload nearly all PP
  * pairs are far.  Sums accumulate in FP32 over groups of 16 interactions
  * (near) or 32 (far), folded into Kahan-compensated totals.
  */
@@ -43,9 +43,10 @@ __device__ __forceinline__ uint32_t lanemask_lt_pp() {
     return r;
 }
 
-/* two staged sources (even, odd) in the far form: negated FP32 offsets */
-struct __align__(8) FarPair {
-    float2 x, y, z;
+/* four staged sources in the far form: negated FP32 offsets, one 16-byte
+ * load per axis for four interactions */
+struct __align__(16) FarQuad {
+    float4 x, y, z;
 };
 
 /* gap between the intervals [a0, a1] and [b0, b1] of fixed-point coordinates
@@ -60,10 +61,10 @@ __device__ __forceinline__ double ppb_axis_gap(int32_t a0, int32_t a1, int32_t b
     return (double)g;
 }
 
-/* one far source pair: 2 interactions, no softening possible */
-__device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, const float2 &az, const FarPair &s,
-                                         PPAcc &a) {
-    const float2 dx = __fadd2_rn(ax, s.x), dy = __fadd2_rn(ay, s.y), dz = __fadd2_rn(az, s.z);
+/* two far sources (packed): 2 interactions, no softening possible */
+__device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, const float2 &az, float2 sx, float2 sy,
+                                         float2 sz, PPAcc &a) {
+    const float2 dx = __fadd2_rn(ax, sx), dy = __fadd2_rn(ay, sy), dz = __fadd2_rn(az, sz);
     const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
     const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
     const float2 f = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
@@ -71,6 +72,12 @@ __device__ __forceinline__ void ppb_far2(const float2 &ax, const float2 &ay, con
     a.t0 = __ffma2_rn(dx, f, a.t0);
     a.t1 = __ffma2_rn(dy, f, a.t1);
     a.t2 = __ffma2_rn(dz, f, a.t2);
+}
+__device__ __forceinline__ void ppb_far4(const float2 &ax, const float2 &ay, const float2 &az, const FarQuad &s,
+                                         PPAcc &a) {
+    const float4 x = s.x, y = s.y, z = s.z;
+    ppb_far2(ax, ay, az, make_float2(x.x, x.y), make_float2(y.x, y.y), make_float2(z.x, z.y), a);
+    ppb_far2(ax, ay, az, make_float2(x.z, x.w), make_float2(y.z, y.w), make_float2(z.z, z.w), a);
 }
 
 /* near source pairs [q, q + n) with r^2 <= h^2: the reference's softened
@@ -118,18 +125,18 @@ __device__ __forceinline__ void ppb_near_stage(const GParams &P, float h2, float
     }
 }
 
-/* the far source pairs [q0, q1) of a stage: this copy's share, folded into
- * the compensated totals every 16 source pairs (32 interactions) */
-__device__ __forceinline__ void ppb_far_stage(float m, const FarPair *sy, int q0, int q1, const float2 &ax,
+/* the far source quads [q0, q1) of a stage: this copy's share, folded into
+ * the compensated totals every 8 quads (32 interactions) */
+__device__ __forceinline__ void ppb_far_stage(float m, const FarQuad *sy, int q0, int q1, const float2 &ax,
                                               const float2 &ay, const float2 &az, PPAcc &a) {
     int q = q0;
-    for (; q + 16 <= q1; q += 16) {
+    for (; q + 8 <= q1; q += 8) {
 #pragma unroll
-        for (int u = 0; u < 16; u++) ppb_far2(ax, ay, az, sy[q + u], a);
+        for (int u = 0; u < 8; u++) ppb_far4(ax, ay, az, sy[q + u], a);
         a.fold(m);
     }
     if (q < q1) {
-        for (; q < q1; q++) ppb_far2(ax, ay, az, sy[q], a);
+        for (; q < q1; q++) ppb_far4(ax, ay, az, sy[q], a);
         a.fold(m);
     }
 }
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(PPB_T, PPB_MINB)
     k_pp_leaf(GParams P, const int32_t *__restrict__ leaves, int32_t nleaves, const int32_t *__restrict__ pb,
               const int32_t *__restrict__ pe, const MSrc *__restrict__ ms, const int32_t *__restrict__ aabb,
               const int4 *__restrict__ pos, ListView LV, const double *__restrict__ far, float4 *__restrict__ acc) {
-    __shared__ __align__(16) SrcPair stage[PPB_STAGE / 2]; /* the far form uses the first half */
+    __shared__ __align__(16) SrcPair stage[PPB_STAGE / 2]; /* the far form (FarQuad) uses the first half */
     __shared__ int32_t m_start[PPB_META + 1], m_pb[PPB_META];
     __shared__ int32_t s_nmeta, s_used, s_cursor;
     __shared__ uint32_t s_amag, s_bmag;
@@ -297,29 +304,30 @@ __global__ void __launch_bounds__(PPB_T, PPB_MINB)
                         split_hl(o2, h, l);
                         e[4] = -h, e[10] = -l;
                     } else {
-                        float *e = sf + (q >> 1) * 6 + (q & 1); /* FarPair: x.x x.y y.x y.y z.x z.y */
+                        float *e = sf + (q >> 2) * 12 + (q & 3); /* FarQuad: x[4] y[4] z[4] */
                         e[0] = -__int2float_rn(o0) * 2.3283064365386963e-10f;
-                        e[2] = -__int2float_rn(o1) * 2.3283064365386963e-10f;
-                        e[4] = -__int2float_rn(o2) * 2.3283064365386963e-10f;
+                        e[4] = -__int2float_rn(o1) * 2.3283064365386963e-10f;
+                        e[8] = -__int2float_rn(o2) * 2.3283064365386963e-10f;
                     }
                 }
-            if ((used & 1) && t == 0) { /* pad: a source at 1e30 gives exactly zero terms */
-                if (pass == 0) {
-                    float *e = sf + (used >> 1) * 12 + 1;
-                    e[0] = -1.0e30f;
-                    e[2] = e[4] = e[6] = e[8] = e[10] = 0.0f;
-                } else {
-                    float *e = sf + (used >> 1) * 6 + 1;
-                    e[0] = -1.0e30f;
-                    e[2] = e[4] = 0.0f;
-                }
+            /* pad to a whole pair (near) or quad (far): a source at 1e30 gives exactly zero terms */
+            if (pass == 0 && t == 0 && (used & 1)) {
+                float *e = sf + (used >> 1) * 12 + 1;
+                e[0] = -1.0e30f;
+                e[2] = e[4] = e[6] = e[8] = e[10] = 0.0f;
+            }
+            if (pass == 1 && t < 3 && used + t < ((used + 3) & ~3)) {
+                const int q = used + t;
+                float *e = sf + (q >> 2) * 12 + (q & 3);
+                e[0] = -1.0e30f;
+                e[4] = e[8] = 0.0f;
             }
             atomicMax(&s_bmag, bmag);
             __syncthreads();
-            const int np = (used + 1) >> 1;
+            const int np = pass == 0 ? (used + 1) >> 1 : (used + 3) >> 2; /* pairs (near) or quads (far) */
             const uint32_t amax = s_amag, bmax = s_bmag;
             if (active) {
-                /* copy `phase` takes the contiguous source pairs [q0, q1) */
+                /* copy `phase` takes the contiguous source pairs or quads [q0, q1) */
                 const int q0 = (np * phase) / C, q1 = (np * (phase + 1)) / C;
                 /* both forms give the int32-wrapped (nearest image) separation
                  * when every |a_i - b_j| < 2^31 */
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(PPB_T, PPB_MINB)
                 if (pass == 0 && fits)
                     ppb_near_stage(P, h2, m, stage, q0, q1, A, a);
                 else if (pass == 1 && fits)
-                    ppb_far_stage(m, reinterpret_cast<const FarPair *>(stage), q0, q1, ax, ay, az, a);
+                    ppb_far_stage(m, reinterpret_cast<const FarQuad *>(stage), q0, q1, ax, ay, az, a);
                 else
                     ppb_wrap_stage(P, m, m_start, m_pb, nmeta, pos, phase, C, xi, per, a);
             }
