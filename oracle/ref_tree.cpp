@@ -1,0 +1,246 @@
+/*
+ * ref_tree.cpp -- runs the reference's own tree build, multipoles and walk
+ * (src/tree.cpp: refine :122-196, compute_multipoles, kick_fmm :384-635)
+ * with its own particle store (src/part_vect.cpp) and kernels
+ * (src/gravity.cpp), all compiled where they lie by oracle/Makefile (target
+ * `reftree`) against the serial HPX stand-in oracle/hpx_shim.  TEST
+ * INFRASTRUCTURE ONLY: it pins the oracle's restated tree and walk
+ * (tg_oracle.cpp) to the reference's code.  Output goes to oracle/_ref/.
+ *
+ * One call = the reference's solve_gravity (src/main.cpp:31-73) on a fresh
+ * tree built as its main loop builds it (src/main.cpp:201-207): refine until
+ * no node splits, compute_multipoles(rung 0, output on), kick_fmm from the
+ * root check item, then part_vect_kick_return.  Every particle is an output
+ * particle, so the kick's output records carry each particle's FP32 phi and
+ * g; the particle's input index travels in its group field (groups are off).
+ * The kernels cache the options of their first call (src/gravity.cpp:
+ * 176-187): one library copy per parameter set.  With `record`, every kernel
+ * call of the walk is recorded (below) for comparison with the oracle's lists.
+ */
+#include <tigergrav/cosmo.hpp>
+#include <tigergrav/gravity.hpp>
+#include <tigergrav/groups.hpp>
+#include <tigergrav/map.hpp>
+#include <tigergrav/options.hpp>
+#include <tigergrav/part_vect.hpp>
+#include <tigergrav/tree.hpp>
+
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+options options::global;
+options &options::get() { return global; }
+void options::set(options o) { global = o; }
+
+/* the particle set part_vect_init loads (initialize.hpp): the caller's positions */
+static std::vector<particle> g_init;
+part_vect initial_particle_set(std::string, int, int) { return g_init; }
+
+/* sky maps and groups are off (opts.map, opts.groups): src/map.cpp and
+ * src/groups.cpp (Silo, HEALPix) are not built, and these are never reached */
+void map_add_particle(const vect<double> &, double, double) { std::abort(); }
+void groups_add_finder(std::function<bool(void)>) { std::abort(); }
+void groups_add_particle1(particle) { std::abort(); }
+void groups_add_particle2(particle) { std::abort(); }
+
+/*
+ * The reference's interaction lists as its walk hands them to the kernels:
+ * tree.cpp is compiled with each gravity_XX_yy renamed to reftree_XX_yy (the
+ * Makefile's -D flags), so every kernel call of kick_fmm lands here, is
+ * recorded (the sink: its first particle, or the node centre; the sources in
+ * call order: particle positions, or multipole centres) and passed on to the
+ * reference's kernel.  Kinds as the oracle numbers its lists: CC_D 0, CP_D 1,
+ * CC_E 2, CP_E 3, PC_D 4, PP_D 5, PC_E 6, PP_E 7.
+ */
+struct CallRec {
+    int kind;
+    int32_t sink[3];
+    int64_t nsink;
+    std::vector<int32_t> src; /* 3 per source */
+};
+static std::vector<CallRec> g_calls;
+static bool g_record = false;
+
+template <class V>
+static void rec_pos(int kind, const int32_t *sink, int64_t nsink, const V &y) {
+    if (!g_record) return;
+    CallRec r{kind, {sink[0], sink[1], sink[2]}, nsink, {}};
+    r.src.reserve(3 * y.size());
+    for (const auto &p : y)
+        for (int d = 0; d < 3; d++) r.src.push_back(p[d]);
+    g_calls.push_back(std::move(r));
+}
+static void rec_multi(int kind, const int32_t *sink, int64_t nsink, const std::vector<multi_src> &y) {
+    if (!g_record) return;
+    CallRec r{kind, {sink[0], sink[1], sink[2]}, nsink, {}};
+    r.src.reserve(3 * y.size());
+    for (const auto &m : y)
+        for (int d = 0; d < 3; d++) r.src.push_back(m.x[d]);
+    g_calls.push_back(std::move(r));
+}
+static void first_of(const std::vector<vect<pos_type>> &x, int32_t *s) {
+    for (int d = 0; d < 3; d++) s[d] = x.empty() ? 0 : x[0][d];
+}
+static void of(const vect<pos_type> &x, int32_t *s) {
+    for (int d = 0; d < 3; d++) s[d] = x[d];
+}
+
+std::uint64_t reftree_PP_direct(std::vector<force> &f, const std::vector<vect<pos_type>> &x,
+                                std::vector<vect<pos_type>> y, bool do_phi) {
+    int32_t s[3];
+    first_of(x, s);
+    rec_pos(5, s, (int64_t)x.size(), y);
+    return gravity_PP_direct(f, x, std::move(y), do_phi);
+}
+std::uint64_t reftree_PP_ewald(std::vector<force> &f, const std::vector<vect<pos_type>> &x,
+                               std::vector<vect<pos_type>> y) {
+    int32_t s[3];
+    first_of(x, s);
+    rec_pos(7, s, (int64_t)x.size(), y);
+    return gravity_PP_ewald(f, x, std::move(y));
+}
+std::uint64_t reftree_PC_direct(std::vector<force> &f, const std::vector<vect<pos_type>> &x,
+                                std::vector<multi_src> &y) {
+    int32_t s[3];
+    first_of(x, s);
+    rec_multi(4, s, (int64_t)x.size(), y);
+    return gravity_PC_direct(f, x, y);
+}
+std::uint64_t reftree_PC_ewald(std::vector<force> &f, const std::vector<vect<pos_type>> &x,
+                               std::vector<multi_src> &y) {
+    int32_t s[3];
+    first_of(x, s);
+    rec_multi(6, s, (int64_t)x.size(), y);
+    return gravity_PC_ewald(f, x, y);
+}
+std::uint64_t reftree_CC_direct(expansion<double> &L, const vect<pos_type> &x, std::vector<multi_src> &y) {
+    int32_t s[3];
+    of(x, s);
+    rec_multi(0, s, 1, y);
+    return gravity_CC_direct(L, x, y);
+}
+std::uint64_t reftree_CC_ewald(expansion<double> &L, const vect<pos_type> &x, std::vector<multi_src> &y) {
+    int32_t s[3];
+    of(x, s);
+    rec_multi(2, s, 1, y);
+    return gravity_CC_ewald(L, x, y);
+}
+std::uint64_t reftree_CP_direct(expansion<double> &L, const vect<pos_type> &x, std::vector<vect<pos_type>> y) {
+    int32_t s[3];
+    of(x, s);
+    rec_pos(1, s, 1, y);
+    return gravity_CP_direct(L, x, std::move(y));
+}
+std::uint64_t reftree_CP_ewald(expansion<double> &L, const vect<pos_type> &x, std::vector<vect<pos_type>> y) {
+    int32_t s[3];
+    of(x, s);
+    rec_pos(3, s, 1, y);
+    return gravity_CP_ewald(L, x, std::move(y));
+}
+
+/* the recorded calls of the last solve: count, then per call its kind, sink
+ * (first particle or node centre), sink count and sources */
+extern "C" int64_t reftree_num_calls() { return (int64_t)g_calls.size(); }
+extern "C" int64_t reftree_call_size(int64_t k) {
+    return k < 0 || k >= (int64_t)g_calls.size() ? -1 : (int64_t)g_calls[(size_t)k].src.size() / 3;
+}
+extern "C" int reftree_get_call(int64_t k, int32_t *kind, int32_t *sink, int64_t *nsink, int32_t *src) {
+    if (k < 0 || k >= (int64_t)g_calls.size()) return -1;
+    const CallRec &r = g_calls[(size_t)k];
+    *kind = r.kind;
+    for (int d = 0; d < 3; d++) sink[d] = r.sink[d];
+    *nsink = r.nsink;
+    std::memcpy(src, r.src.data(), sizeof(int32_t) * r.src.size());
+    return 0;
+}
+
+/* the kick's output records are kept between calls by the reference
+ * (kick_rc); the driver reads them after each solve and clears them */
+extern kick_return kick_rc;
+
+static bool g_inited = false;
+static double g_key[7];
+
+extern "C" int reftree_solve(const int32_t *x, int64_t n, double theta, int ewald, int leaf_max, double soft_len,
+                             double G, int record, float *phi, float *g, uint64_t *istats, int64_t *tree_counts) {
+    const double key[7] = {theta, (double)ewald, (double)leaf_max, soft_len, G, (double)n, 1.0};
+    if (g_inited && std::memcmp(key, g_key, sizeof(key)) != 0) return -1; /* one parameter set per copy */
+    options o = options();
+    o.problem = "caller";
+    o.problem_size = (std::uint64_t)n;
+    o.out_parts = (int)n;
+    o.theta = theta;
+    o.ewald = ewald != 0;
+    o.parts_per_node = leaf_max;
+    o.soft_len = soft_len;
+    o.m_tot = 1.0;
+    o.G = G;
+    o.gravity = true;
+    o.solver_test = false;
+    o.cosmic = false;
+    o.glass = false;
+    o.groups = false;
+    o.map = false;
+    o.balanced_tree = false;
+    o.workgroup_size = 32;
+    o.oversubscription = 1;
+    o.dt_max = 1.0 / 64.0;
+    o.t_max = 1.0;
+    o.eta = 0.2;
+    o.nout = 1;
+    options::set(o);
+    std::memcpy(g_key, key, sizeof(key));
+    g_inited = true;
+
+    g_init.assign((size_t)n, particle());
+    for (int64_t i = 0; i < n; i++) {
+        particle &p = g_init[(size_t)i];
+        for (int d = 0; d < 3; d++) {
+            p.x[d] = x[3 * i + d];
+            p.v[d] = 0.0f;
+        }
+        p.flags.out = 1;
+        p.flags.rung = 0;
+        p.flags.group = (std::uint64_t)i;
+    }
+    cosmo_init(1.0, 0.0);
+    part_vect_init();
+    tree::set_theta(theta);
+    tree_client root = hpx::new_<tree>(hpx::find_here(), 1, 0, (part_iter)n, 0).get();
+    refine_return rr;
+    do {
+        rr = root.refine(0);
+    } while (rr.rc);
+    tree_counts[0] = (int64_t)rr.nodes;
+    tree_counts[1] = (int64_t)rr.leaves;
+    kick_rc.out.clear();
+    kick_rc.rung = 0;
+    kick_rc.stats.zero();
+    g_calls.clear();
+    g_record = record != 0;
+    root.compute_multipoles(0, true, 0);
+    auto root_list = std::vector<check_item>(1, root.get_check_item());
+    expansion<double> L;
+    L = 0.0;
+    const interaction_stats st = root.kick_fmm(root_list, root_list, {{0.5, 0.5, 0.5}}, L, 0, true, 0);
+    const kick_return rc = part_vect_kick_return();
+    g_record = false;
+    istats[0] = st.PP_direct;
+    istats[1] = st.PP_ewald;
+    istats[2] = st.CC_direct;
+    istats[3] = st.CC_ewald;
+    istats[4] = st.CP_direct;
+    istats[5] = st.CP_ewald;
+    int64_t seen = 0;
+    for (const output &out : rc.out) {
+        const std::uint64_t i = out.id;
+        if (i >= (std::uint64_t)n) return -2;
+        phi[i] = out.phi;
+        for (int d = 0; d < 3; d++) g[3 * i + d] = out.g[d];
+        seen++;
+    }
+    kick_rc.out.clear();
+    hpx::release_components();
+    return seen == n ? 0 : -3;
+}

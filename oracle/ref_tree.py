@@ -1,0 +1,100 @@
+"""The reference's own tree build and walk, run on the host (TEST
+INFRASTRUCTURE ONLY).
+
+oracle/_ref/libtg_reftree.so is src/tree.cpp, src/part_vect.cpp,
+src/gravity.cpp, src/cosmo.cpp and src/range.cpp of the reference, compiled
+where they lie by oracle/Makefile (target `reftree`) against the serial HPX
+stand-in oracle/hpx_shim, with the driver oracle/ref_tree.cpp: one call is the
+reference's solve_gravity (src/main.cpp:31-73) on a tree refined as its main
+loop refines it (src/main.cpp:201-207).  It gives the FP32 phi and g of every
+particle (the kick's output records), the interaction statistics of kick_fmm,
+the node and leaf counts of refine, and every kernel call of the walk with its
+sink and sources in call order, for checking the oracle's restated tree and
+walk (and through them the CUDA path) against the reference's code.
+
+The reference caches options in function-local statics (src/gravity.cpp:
+176-187, src/tree.cpp), so one loaded library serves one parameter set per
+process; further parameter sets load their own copies of the file.
+"""
+from __future__ import annotations
+
+import atexit
+import ctypes as C
+import os
+import shutil
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(HERE, "_ref", "libtg_reftree.so")
+KIND_NAMES = ("CC_D", "CP_D", "CC_E", "CP_E", "PC_D", "PP_D", "PC_E", "PP_E")
+
+_libs: dict = {}
+_tmp = None
+
+
+def available() -> bool:
+    return os.path.exists(PATH)
+
+
+def _lib(key):
+    global _tmp
+    if key not in _libs:
+        path = PATH
+        if _libs:
+            if _tmp is None:
+                _tmp = tempfile.mkdtemp(prefix="tg_reftree_")
+                atexit.register(shutil.rmtree, _tmp, True)
+            path = os.path.join(_tmp, "libtg_reftree_%d.so" % len(_libs))
+            shutil.copyfile(PATH, path)
+        L = C.CDLL(path)
+        L.reftree_solve.restype = C.c_int
+        L.reftree_solve.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.reftree_num_calls.restype = C.c_int64
+        L.reftree_call_size.restype = C.c_int64
+        L.reftree_call_size.argtypes = [C.c_int64]
+        L.reftree_get_call.restype = C.c_int
+        L.reftree_get_call.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _libs[key] = L
+    return _libs[key]
+
+
+def solve(x: np.ndarray, theta: float, ewald: bool, leaf_max: int = 64, soft_len: float | None = None,
+          G: float = 1.0, record: bool = False) -> dict:
+    """The reference's solve of int32 fixed-point positions x (n x 3), m = 1/n,
+    soft_len 0.02 n^-1/3 unless given.  Returns phi (n, FP32), g (n x 3,
+    FP32), stats (the six interaction_stats counters), nodes, leaves and, with
+    record, calls: (kind, sink, nsink, sources) per kernel call with sources,
+    sink = the first sink particle (leaf kinds) or the node centre, sources =
+    positions or multipole centres as an (m x 3) int32 array."""
+    x = np.ascontiguousarray(x, np.int32)
+    n = len(x)
+    if soft_len is None:
+        soft_len = 0.02 * n ** (-1.0 / 3.0)
+    key = (float(theta), int(bool(ewald)), int(leaf_max), float(soft_len), float(G), int(n))
+    L = _lib(key)
+    phi = np.zeros(n, np.float32)
+    g = np.zeros((n, 3), np.float32)
+    st = np.zeros(6, np.uint64)
+    tc = np.zeros(2, np.int64)
+    rc = L.reftree_solve(x.ctypes.data, n, float(theta), int(bool(ewald)), int(leaf_max), float(soft_len), float(G),
+                         int(bool(record)), phi.ctypes.data, g.ctypes.data, st.ctypes.data, tc.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_solve: %d" % rc)
+    out = dict(phi=phi, g=g, nodes=int(tc[0]), leaves=int(tc[1]),
+               stats=dict(zip(("PP_direct", "PP_ewald", "CC_direct", "CC_ewald", "CP_direct", "CP_ewald"),
+                              map(int, st))))
+    if record:
+        calls = []
+        kind = np.zeros(1, np.int32)
+        sink = np.zeros(3, np.int32)
+        ns = np.zeros(1, np.int64)
+        for k in range(L.reftree_num_calls()):
+            m = L.reftree_call_size(k)
+            src = np.zeros((max(m, 1), 3), np.int32)
+            L.reftree_get_call(k, kind.ctypes.data, sink.ctypes.data, ns.ctypes.data, src.ctypes.data)
+            calls.append((KIND_NAMES[int(kind[0])], tuple(int(v) for v in sink), int(ns[0]), src[:m].copy()))
+        out["calls"] = calls
+    return out

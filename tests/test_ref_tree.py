@@ -1,0 +1,108 @@
+"""The oracle's tree and walk against the reference's own (src/tree.cpp run on
+the host through oracle/_ref/libtg_reftree.so): node and leaf counts, the
+interaction statistics, every list of every node in content and order (as
+the reference's walk hands them to its kernels), and the forces of a whole
+solve with the reference's kernels.  The CUDA path's trees and lists are
+bit-identical to the oracle's (tests/test_gpu_path.py,
+tests/test_parity_config1.py), so these pin them to the reference's code.
+
+Needs the reference sources at build time (oracle/Makefile `reftree`);
+skipped where the library was not built.
+"""
+import numpy as np
+import pytest
+
+import ref_tree
+
+pytestmark = pytest.mark.skipif(not ref_tree.available(), reason="oracle/_ref/libtg_reftree.so not built")
+
+CASES = {
+    "clustered16_free_t07": dict(kind="clustered", nside=16, theta=0.7, ewald=False, leaf=64),
+    "clustered16_free_t03_leaf16": dict(kind="clustered", nside=16, theta=0.3, ewald=False, leaf=16),
+    "uniform2048_ewald_t05": dict(kind="uniform", n=2048, theta=0.5, ewald=True, leaf=64),
+    "clustered12_ewald_t07_leaf24": dict(kind="clustered", nside=12, theta=0.7, ewald=True, leaf=24),
+}
+
+_solved = {}
+
+
+def _case(name, oracle_mod):
+    if name not in _solved:
+        from tigergrav_b200 import ics
+        c = CASES[name]
+        x = ics.clustered(c["nside"], 3) if c["kind"] == "clustered" else ics.uniform(c["n"], 1)
+        r = ref_tree.solve(x, c["theta"], c["ewald"], c["leaf"], record=True)
+        o = oracle_mod.Oracle(theta=c["theta"], ewald=c["ewald"], leaf_max=c["leaf"]).set_particles(x)
+        o.build().multipoles().walk()
+        _solved[name] = (x, r, o)
+    return _solved[name]
+
+
+def _oracle_calls(x, o):
+    """the oracle's lists in the form the reference's walk calls its kernels"""
+    nd = o.nodes()
+    xs = x[o.perm()]
+    out = []
+    for name in ref_tree.KIND_NAMES:
+        off, ids = o.list(name)
+        for i in range(o.num_nodes):
+            lst = ids[off[i]:off[i + 1]]
+            if len(lst) == 0:
+                continue
+            pb, pe = nd["pbegin"][i], nd["pend"][i]
+            if name in ("PC_D", "PP_D", "PC_E", "PP_E"):
+                sink, ns = tuple(int(v) for v in xs[pb]), int(pe - pb)
+            else:
+                sink, ns = tuple(int(v) for v in nd["x"][i]), 1
+            if name in ("CC_D", "CC_E", "PC_D", "PC_E"):
+                src = nd["x"][lst]
+            else:
+                src = np.concatenate([xs[nd["pbegin"][j]:nd["pend"][j]] for j in lst])
+            if len(src):
+                out.append((name, sink, ns, src.astype(np.int32)))
+    return out
+
+
+def _key(c):
+    return (c[0], c[1], c[2], c[3].tobytes())
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_tree_counts_and_stats_match_reference(name, oracle_mod):
+    x, r, o = _case(name, oracle_mod)
+    nd = o.nodes()
+    assert r["nodes"] == o.num_nodes
+    assert r["leaves"] == int((nd["child0"] < 0).sum())
+    ref_stats, _, _ = o.stats()
+    assert r["stats"] == ref_stats
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_lists_match_reference_walk(name, oracle_mod):
+    """every kernel call of the reference's kick_fmm that has sources is one
+    of the oracle's lists (same sink, same sources in the same order), and
+    the other way round"""
+    x, r, o = _case(name, oracle_mod)
+    ref = sorted(_key(c) for c in r["calls"] if len(c[3]))
+    mine = sorted(_key(c) for c in _oracle_calls(x, o))
+    assert len(ref) == len(mine)
+    assert ref == mine
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_forces_match_reference_solve(name, oracle_mod, has_ref):
+    """the whole solve: the oracle's lists through the reference's kernels
+    against the reference's own run, to the last bits of FP32 (the expansion
+    arithmetic of L2L / L2P is restated in the oracle, and the reference's
+    build contracts it into FMAs)"""
+    if not has_ref:
+        pytest.skip("reference kernels not built")
+    x, r, o = _case(name, oracle_mod)
+    o.evaluate(use_ref=True)
+    phi, g = o.forces()
+    gn = np.linalg.norm(g, axis=1)
+    eg = np.linalg.norm(r["g"].astype(np.float64) - g, axis=1) / gn
+    ep = np.abs(r["phi"].astype(np.float64) - phi) / np.abs(phi).max()
+    assert eg.max() <= 1e-6, eg.max()
+    assert ep.max() <= 1e-6, ep.max()
+    assert np.median(eg) <= 1e-7
