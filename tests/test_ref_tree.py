@@ -39,7 +39,8 @@ def _case(name, oracle_mod):
 
 
 def _oracle_calls(x, o):
-    """the oracle's lists in the form the reference's walk calls its kernels"""
+    """the lists of o (the oracle, or the CUDA path's GravitySolver: the same
+    introspection) in the form the reference's walk calls its kernels"""
     nd = o.nodes()
     xs = x[o.perm()]
     out = []
@@ -106,3 +107,21 @@ def test_forces_match_reference_solve(name, oracle_mod, has_ref):
     assert eg.max() <= 1e-6, eg.max()
     assert ep.max() <= 1e-6, ep.max()
     assert np.median(eg) <= 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["clustered16_free_t07", "uniform2048_ewald_t05", "clustered12_ewald_t07_leaf24"])
+def test_gpu_walk_matches_reference_walk(name, oracle_mod):
+    """the CUDA path's tree counts, statistics and lists against the
+    reference's own walk directly"""
+    import tigergrav_b200 as tg
+    x, r, _ = _case(name, oracle_mod)
+    c = CASES[name]
+    with tg.GravitySolver(len(x), theta=c["theta"], ewald=c["ewald"], leaf_max=c["leaf"]) as s:
+        s.set_particles(x).solve_gravity()
+        st = s.stats()
+        assert st["nodes"] == r["nodes"]
+        assert st["ref_stats"] == r["stats"]
+        mine = sorted(_key(q) for q in _oracle_calls(x, s))
+    ref = sorted(_key(q) for q in r["calls"] if len(q[3]))
+    assert ref == mine
