@@ -109,11 +109,103 @@ def test_forces_match_reference_solve(name, oracle_mod, has_ref):
     assert np.median(eg) <= 1e-7
 
 
+def _canonical(x, s, ref_calls):
+    """Both walks in a form that does not depend on the order of particles
+    inside a leaf (the CUDA path sorts the particles of a leaf by Morton key,
+    the reference by its midpoint partition; the leaves and their sets are the
+    same): a leaf sink is named by the node of s that holds its first
+    particle, and particle sources are cut into s's source leaves, each taken
+    as a set.  Returns (reference calls, s's calls) as sorted lists."""
+    nd = s.nodes()
+    perm = s.perm()
+    xs = x[perm]
+    leaf_of = np.full(len(x), -1, np.int64)  # caller index -> leaf of s
+    for i in np.nonzero(nd["child0"] < 0)[0]:
+        leaf_of[perm[nd["pbegin"][i]:nd["pend"][i]]] = i
+    index_of = {tuple(int(v) for v in p): k for k, p in enumerate(x)}
+    mine, cuts = [], {}
+    for name in ref_tree.KIND_NAMES:
+        off, ids = s.list(name)
+        for i in range(s.num_nodes):
+            lst = ids[off[i]:off[i + 1]]
+            if len(lst) == 0:
+                continue
+            leafk = name in ("PC_D", "PP_D", "PC_E", "PP_E")
+            sink = int(i) if leafk else tuple(int(v) for v in nd["x"][i])
+            ns = int(nd["pend"][i] - nd["pbegin"][i]) if leafk else 1
+            if name in ("CC_D", "CC_E", "PC_D", "PC_E"):
+                src = tuple(tuple(int(v) for v in c) for c in nd["x"][lst])
+            else:
+                sizes = [int(nd["pend"][j] - nd["pbegin"][j]) for j in lst]
+                cuts[(name, sink)] = sizes
+                src = tuple(tuple(sorted(tuple(int(v) for v in p) for p in xs[nd["pbegin"][j]:nd["pend"][j]]))
+                            for j in lst)
+            if len(src):
+                mine.append((name, sink, ns, src))
+    ref = []
+    for name, first, ns, src in ref_calls:
+        if len(src) == 0:
+            continue
+        leafk = name in ("PC_D", "PP_D", "PC_E", "PP_E")
+        sink = int(leaf_of[index_of[first]]) if leafk else first
+        pts = [tuple(int(v) for v in p) for p in src]
+        if name in ("CC_D", "CC_E", "PC_D", "PC_E"):
+            can = tuple(pts)
+        else:
+            sizes = cuts.get((name, sink), [len(pts)])
+            if sum(sizes) != len(pts):
+                sizes = [len(pts)]
+            can, k = [], 0
+            for n in sizes:
+                can.append(tuple(sorted(pts[k:k + n])))
+                k += n
+            can = tuple(can)
+        ref.append((name, sink, ns, can))
+    return sorted(ref), sorted(mine)
+
+
+@pytest.mark.parametrize("name", ["clustered12_ewald_t07_leaf24"])
+def test_canonical_form_ignores_the_order_inside_leaves(name, oracle_mod):
+    """the comparison the GPU test below makes, on the oracle with the
+    particles of every leaf put in another order: it still matches, and a
+    changed list does not"""
+    x, r, o = _case(name, oracle_mod)
+
+    class Shuffled:
+        num_nodes = o.num_nodes
+
+        def __init__(self):
+            self.nd = o.nodes()
+            p = o.perm().copy()
+            rng = np.random.default_rng(5)
+            for i in np.nonzero(self.nd["child0"] < 0)[0]:
+                b, e = self.nd["pbegin"][i], self.nd["pend"][i]
+                p[b:e] = p[b:e][rng.permutation(e - b)]
+            self.p = p
+
+        def nodes(self):
+            return self.nd
+
+        def perm(self):
+            return self.p
+
+        def list(self, kind):
+            return o.list(kind)
+
+    ref, mine = _canonical(x, Shuffled(), r["calls"])
+    assert ref == mine
+    bad = [c for c in r["calls"] if c[0] == "PP_D" and len(c[3]) > 1][0]
+    calls = [c for c in r["calls"] if c is not bad] + [(bad[0], bad[1], bad[2], bad[3][:-1])]
+    ref2, _ = _canonical(x, Shuffled(), calls)
+    assert ref2 != mine
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["clustered16_free_t07", "uniform2048_ewald_t05", "clustered12_ewald_t07_leaf24"])
 def test_gpu_walk_matches_reference_walk(name, oracle_mod):
     """the CUDA path's tree counts, statistics and lists against the
-    reference's own walk directly"""
+    reference's own walk directly (the lists' sources in order, the particles
+    of each leaf as a set)"""
     import tigergrav_b200 as tg
     x, r, _ = _case(name, oracle_mod)
     c = CASES[name]
@@ -122,6 +214,6 @@ def test_gpu_walk_matches_reference_walk(name, oracle_mod):
         st = s.stats()
         assert st["nodes"] == r["nodes"]
         assert st["ref_stats"] == r["stats"]
-        mine = sorted(_key(q) for q in _oracle_calls(x, s))
-    ref = sorted(_key(q) for q in r["calls"] if len(q[3]))
+        ref, mine = _canonical(x, s, r["calls"])
+    assert len(ref) == len(mine)
     assert ref == mine
