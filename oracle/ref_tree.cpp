@@ -155,6 +155,74 @@ extern "C" int reftree_get_call(int64_t k, int32_t *kind, int32_t *sink, int64_t
     return 0;
 }
 
+/*
+ * The reference's cosmology (src/cosmo.cpp, compiled into this library):
+ * cosmos::advance_to_time on a given state, and the sequence of
+ * cosmo_advance steps with the factors it leaves behind (the scale factors
+ * of cosmo_scale, the float time, kick_dt1 / kick_dt2 per rung and the drift
+ * factor).  cosmo_advance's rung steps use rung_to_dt, whose t_max the
+ * reference caches on first use (tigergrav/time.hpp): this library's solves
+ * and these calls all use t_max = 1.
+ */
+extern double kick_dt1[RUNG_MAX + 1];
+extern double kick_dt2[RUNG_MAX + 1];
+extern float this_time;
+extern double drift_dt;
+
+static void cosmo_options(double H0, double omega_m, double omega_lambda, int cosmic) {
+    options o = options::get();
+    o.H0 = H0;
+    o.omega_m = omega_m;
+    o.omega_lambda = omega_lambda;
+    o.cosmic = cosmic != 0;
+    o.t_max = 1.0;
+    options::set(o);
+}
+
+/* out: a, adot, tau, drift_dt, kick_dt after advance_to_time(t0) from (a, adot, tau) */
+extern "C" void reftree_cosmos_advance(double a, double adot, double tau, double t0, double H0, double omega_m,
+                                       double omega_lambda, double *out) {
+    cosmo_options(H0, omega_m, omega_lambda, 1);
+    cosmos c(a, adot, tau);
+    c.advance_to_time(t0);
+    out[0] = c.get_scale();
+    out[1] = c.get_Hubble() * c.get_scale();
+    out[2] = c.get_tau();
+    out[3] = c.get_drift_dt();
+    out[4] = c.get_kick_dt();
+}
+
+/* cosmo_init(a0, adot0) with the reference's starting values (its globals as
+ * a fresh run has them: kick_dt1 = kick_dt2 = {-1, 0, ...}, time 0, drift 0),
+ * then one cosmo_advance per dt; per step out holds 5 + 2 (RUNG_MAX + 1) doubles:
+ * the scale factor before and after (cosmo_scale), the float time, tau,
+ * drift_dt, then kick_dt1[0..RUNG_MAX] and kick_dt2[0..RUNG_MAX] */
+extern "C" int reftree_cosmo_steps(double a0, double adot0, double H0, double omega_m, double omega_lambda,
+                                   const double *dts, int nsteps, double *out) {
+    cosmo_options(H0, omega_m, omega_lambda, 1);
+    for (int i = 0; i <= RUNG_MAX; i++) kick_dt1[i] = kick_dt2[i] = 0.0;
+    kick_dt1[0] = kick_dt2[0] = -1.0;
+    this_time = 0.0f;
+    drift_dt = 0.0;
+    cosmo_init(a0, adot0);
+    const int W = 5 + 2 * (RUNG_MAX + 1);
+    for (int k = 0; k < nsteps; k++) {
+        cosmo_advance(dts[k]);
+        double *o = out + (size_t)k * W;
+        const auto sc = cosmo_scale();
+        o[0] = sc.first;
+        o[1] = sc.second;
+        o[2] = this_time;
+        o[3] = cosmo_time();
+        o[4] = cosmo_drift_dt();
+        for (int i = 0; i <= RUNG_MAX; i++) {
+            o[5 + i] = cosmo_kick_dt1((rung_type)i);
+            o[5 + RUNG_MAX + 1 + i] = cosmo_kick_dt2((rung_type)i);
+        }
+    }
+    return 0;
+}
+
 /* the kick's output records are kept between calls by the reference
  * (kick_rc); the driver reads them after each solve and clears them */
 extern kick_return kick_rc;

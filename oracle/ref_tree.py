@@ -10,7 +10,8 @@ loop refines it (src/main.cpp:201-207).  It gives the FP32 phi and g of every
 particle (the kick's output records), the interaction statistics of kick_fmm,
 the node and leaf counts of refine, and every kernel call of the walk with its
 sink and sources in call order, for checking the oracle's restated tree and
-walk (and through them the CUDA path) against the reference's code.
+walk (and through them the CUDA path) against the reference's code; and the
+reference's cosmology (src/cosmo.cpp) for the oracle's restatement of it.
 
 The reference caches options in function-local statics (src/gravity.cpp:
 176-187, src/tree.cpp), so one loaded library serves one parameter set per
@@ -57,6 +58,10 @@ def _lib(key):
         L.reftree_call_size.argtypes = [C.c_int64]
         L.reftree_get_call.restype = C.c_int
         L.reftree_get_call.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.reftree_cosmos_advance.restype = None
+        L.reftree_cosmos_advance.argtypes = [C.c_double] * 7 + [C.c_void_p]
+        L.reftree_cosmo_steps.restype = C.c_int
+        L.reftree_cosmo_steps.argtypes = [C.c_double] * 5 + [C.c_void_p, C.c_int, C.c_void_p]
         _libs[key] = L
     return _libs[key]
 
@@ -98,3 +103,30 @@ def solve(x: np.ndarray, theta: float, ewald: bool, leaf_max: int = 64, soft_len
             calls.append((KIND_NAMES[int(kind[0])], tuple(int(v) for v in sink), int(ns[0]), src[:m].copy()))
         out["calls"] = calls
     return out
+
+
+RUNG_MAX = 30
+
+
+def cosmos_advance(state, t0, H0, omega_m, omega_lambda):
+    """The reference's cosmos::advance_to_time (src/cosmo.cpp:50-106) from
+    state = (a, adot, tau): returns ([a, adot, tau], drift_dt, kick_dt)."""
+    out = np.zeros(5)
+    _lib("cosmo").reftree_cosmos_advance(float(state[0]), float(state[1]), float(state[2]), float(t0), float(H0),
+                                         float(omega_m), float(omega_lambda), out.ctypes.data)
+    return [out[0], out[1], out[2]], out[3], out[4]
+
+
+def cosmo_steps(a0, adot0, dts, H0, omega_m, omega_lambda) -> list:
+    """The reference's cosmo_init(a0, adot0) and one cosmo_advance per dt
+    (src/cosmo.cpp:187-232, t_max = 1): per step a dict of a_last, a, the
+    float time, tau, drift, kick1 and kick2 (RUNG_MAX + 1 each)."""
+    dts = np.ascontiguousarray(dts, np.float64)
+    W = 5 + 2 * (RUNG_MAX + 1)
+    out = np.zeros((len(dts), W))
+    rc = _lib("cosmo").reftree_cosmo_steps(float(a0), float(adot0), float(H0), float(omega_m), float(omega_lambda),
+                                          dts.ctypes.data, len(dts), out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_cosmo_steps: %d" % rc)
+    return [dict(a_last=o[0], a=o[1], time=o[2], tau=o[3], drift=o[4], kick1=o[5:5 + RUNG_MAX + 1],
+                 kick2=o[5 + RUNG_MAX + 1:]) for o in out]
