@@ -227,6 +227,88 @@ extern "C" int reftree_cosmo_steps(double a0, double adot0, double H0, double om
  * (kick_rc); the driver reads them after each solve and clears them */
 extern kick_return kick_rc;
 
+/*
+ * The reference's rung kick and drift on given particles (src/part_vect.cpp:
+ * part_vect_kick :341-436, part_vect_drift :493-540), with forces the caller
+ * supplies: the particle store is loaded as part_vect_init loads it, the
+ * call runs, and the store is read back (part_vect_read).  No cosmology, no
+ * glass, Ewald off (so the second half-kick is the plain 0.5 dt).  t_max = 1.
+ * part_vect_drift caches its options on first use: one parameter set per
+ * library copy.
+ */
+static void load_particles(const int32_t *x, const float *v, const int8_t *rung, int64_t n, double dt_max,
+                           double eta, double soft_len, double G) {
+    options o = options();
+    o.problem = "caller";
+    o.problem_size = (std::uint64_t)n;
+    o.out_parts = (int)n;
+    o.m_tot = 1.0;
+    o.G = G;
+    o.dt_max = dt_max;
+    o.eta = eta;
+    o.soft_len = soft_len;
+    o.t_max = 1.0;
+    o.theta = 0.7;
+    o.parts_per_node = 64;
+    o.ewald = false;
+    o.cosmic = false;
+    o.glass = false;
+    o.groups = false;
+    o.map = false;
+    options::set(o);
+    g_init.assign((size_t)n, particle());
+    for (int64_t i = 0; i < n; i++) {
+        particle &p = g_init[(size_t)i];
+        for (int d = 0; d < 3; d++) {
+            p.x[d] = x[3 * i + d];
+            p.v[d] = v[3 * i + d];
+        }
+        p.flags.out = 1;
+        p.flags.rung = rung ? (std::uint64_t)rung[i] : 0;
+        p.flags.group = (std::uint64_t)i;
+    }
+    cosmo_init(1.0, 0.0);
+    part_vect_init();
+}
+
+/* part_vect_kick(0, n, min_rung, do_out, f) with f = g of the particles it
+ * takes (rung >= min_rung, or all with do_out), in order; v, rungs and the
+ * largest new rung out */
+extern "C" int reftree_kick(const int32_t *x, const float *v, const int8_t *rung, const float *g, int64_t n,
+                            int min_rung, int do_out, double dt_max, double eta, double soft_len, double G,
+                            float *v_out, int8_t *rung_out, int32_t *max_rung) {
+    load_particles(x, v, rung, n, dt_max, eta, soft_len, G);
+    std::vector<force> f;
+    for (int64_t i = 0; i < n; i++)
+        if (rung[i] >= min_rung || do_out) {
+            force q;
+            q.phi = 0.0f;
+            for (int d = 0; d < 3; d++) q.g[d] = g[3 * i + d];
+            f.push_back(q);
+        }
+    kick_rc.out.clear();
+    kick_rc.rung = 0;
+    part_vect_kick(0, (part_iter)n, (rung_type)min_rung, do_out != 0, std::move(f)).get();
+    *max_rung = kick_rc.rung;
+    kick_rc.out.clear();
+    const std::vector<particle> ps = part_vect_read(0, (part_iter)n).get();
+    for (int64_t i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) v_out[3 * i + d] = ps[(size_t)i].v[d];
+        rung_out[i] = (int8_t)ps[(size_t)i].flags.rung;
+    }
+    return 0;
+}
+
+/* part_vect_drift(0, mrung): every particle moves by v rung_to_dt(mrung), wrapped into the box */
+extern "C" int reftree_drift(const int32_t *x, const float *v, int64_t n, int mrung, int32_t *x_out) {
+    load_particles(x, v, nullptr, n, 1.0, 0.2, 0.01, 1.0);
+    part_vect_drift(0.0, (rung_type)mrung);
+    const std::vector<particle> ps = part_vect_read(0, (part_iter)n).get();
+    for (int64_t i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) x_out[3 * i + d] = ps[(size_t)i].x[d];
+    return 0;
+}
+
 static bool g_inited = false;
 static double g_key[7];
 

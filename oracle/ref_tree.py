@@ -60,6 +60,11 @@ def _lib(key):
         L.reftree_get_call.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.reftree_cosmos_advance.restype = None
         L.reftree_cosmos_advance.argtypes = [C.c_double] * 7 + [C.c_void_p]
+        L.reftree_kick.restype = C.c_int
+        L.reftree_kick.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int, C.c_int] + [C.c_double] * 4 + \
+            [C.c_void_p] * 3
+        L.reftree_drift.restype = C.c_int
+        L.reftree_drift.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         L.reftree_cosmo_steps.restype = C.c_int
         L.reftree_cosmo_steps.argtypes = [C.c_double] * 5 + [C.c_void_p, C.c_int, C.c_void_p]
         _libs[key] = L
@@ -130,3 +135,36 @@ def cosmo_steps(a0, adot0, dts, H0, omega_m, omega_lambda) -> list:
         raise RuntimeError("reftree_cosmo_steps: %d" % rc)
     return [dict(a_last=o[0], a=o[1], time=o[2], tau=o[3], drift=o[4], kick1=o[5:5 + RUNG_MAX + 1],
                  kick2=o[5 + RUNG_MAX + 1:]) for o in out]
+
+
+def kick(x, v, rung, g, min_rung, do_out, dt_max, eta, soft_len, G=1.0):
+    """The reference's part_vect_kick (src/part_vect.cpp:341-436) on these
+    particles with accelerations g (float32, per unit G) for the ones it takes:
+    returns (v, rung, largest new rung).  t_max = 1, no cosmology, Ewald off."""
+    x = np.ascontiguousarray(x, np.int32)
+    v = np.ascontiguousarray(v, np.float32)
+    rung = np.ascontiguousarray(rung, np.int8)
+    g = np.ascontiguousarray(g, np.float32)
+    n = len(x)
+    vo = np.zeros((n, 3), np.float32)
+    ro = np.zeros(n, np.int8)
+    mr = np.zeros(1, np.int32)
+    key = ("kick", float(dt_max), float(eta), float(soft_len), float(G))
+    rc = _lib(key).reftree_kick(x.ctypes.data, v.ctypes.data, rung.ctypes.data, g.ctypes.data, n, int(min_rung),
+                                int(bool(do_out)), float(dt_max), float(eta), float(soft_len), float(G), vo.ctypes.data,
+                                ro.ctypes.data, mr.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_kick: %d" % rc)
+    return vo, ro, int(mr[0])
+
+
+def drift(x, v, mrung):
+    """The reference's part_vect_drift (src/part_vect.cpp:493-540) by
+    rung_to_dt(mrung) (t_max = 1): the new int32 positions."""
+    x = np.ascontiguousarray(x, np.int32)
+    v = np.ascontiguousarray(v, np.float32)
+    xo = np.zeros_like(x)
+    rc = _lib(("drift", len(x))).reftree_drift(x.ctypes.data, v.ctypes.data, len(x), int(mrung), xo.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_drift: %d" % rc)
+    return xo

@@ -208,3 +208,53 @@ def test_oracle_stepper_time_line():
     # particle k (rung k + 2) is active every 2^(5 - (k + 2)) steps
     counts = [sum(1 for _, m, _ in seen if m <= r) for r in (2, 3, 4, 5)]
     assert counts == [32 // 8, 32 // 4, 32 // 2, 32]
+
+
+# ---- the restated kick and drift against the reference's own ---------------
+# (src/part_vect.cpp compiled into oracle/_ref/libtg_reftree.so; skipped where
+# it was not built)
+
+def _ref_tree():
+    import ref_tree
+    if not ref_tree.available():
+        pytest.skip("oracle/_ref/libtg_reftree.so not built")
+    return ref_tree
+
+
+@pytest.mark.parametrize("min_rung,do_out", [(0, 0), (0, 1), (1, 0), (1, 1), (3, 0), (3, 1)])
+def test_kick_matches_reference_part_vect_kick(min_rung, do_out):
+    """orung.kick (the rung choice and both half kicks of the active
+    particles) bit for bit against part_vect_kick itself, on accelerations
+    spanning six decades so that the particles spread over many rungs"""
+    rt = _ref_tree()
+    rng = np.random.default_rng(10 + min_rung)
+    n = 3000
+    x = rng.integers(-2 ** 31, 2 ** 31, size=(n, 3), dtype=np.int64).astype(np.int32)
+    v = (rng.standard_normal((n, 3)) * 0.05).astype(np.float32)
+    g = (rng.standard_normal((n, 3)) * 10 ** rng.uniform(-2, 4, (n, 1))).astype(np.float32)
+    rung = np.zeros(n, np.int8) if min_rung == 0 else rng.integers(0, 7, n).astype(np.int8)
+    h, dt_max, eta = 0.02 / 14, 1.0 / 16, 0.2
+    vr, rr, mr = rt.kick(x, v, rung, g, min_rung, do_out, dt_max, eta, h)
+    vo, ro = v.copy(), rung.copy()
+    mo = orung.kick(vo, ro, g, min_rung, 1.0, dt_max, eta, h)
+    np.testing.assert_array_equal(vr, vo)
+    np.testing.assert_array_equal(rr, ro)
+    assert len(np.unique(rr)) >= 8
+    assert mr == mo
+
+
+@pytest.mark.parametrize("mrung", [0, 1, 4, 9])
+def test_drift_matches_reference_part_vect_drift(mrung, oracle_mod):
+    """the oracle's drift (x += v dt in double, wrapped, back to fixed point)
+    bit for bit against part_vect_drift itself, with velocities that wrap
+    particles across the box"""
+    rt = _ref_tree()
+    rng = np.random.default_rng(20 + mrung)
+    n = 5000
+    x = rng.integers(-2 ** 31, 2 ** 31, size=(n, 3), dtype=np.int64).astype(np.int32)
+    v = (rng.standard_normal((n, 3)) * 0.7).astype(np.float32)
+    xr = rt.drift(x, v, mrung)
+    o = oracle_mod.Oracle(theta=0.7).set_particles(x, v)
+    o.drift(1.0 / (1 << mrung))
+    xo, _ = o.particles()
+    np.testing.assert_array_equal(xr, xo)
