@@ -70,8 +70,13 @@ def propagate_labels(x, link_len, periodic=True):
     return np.array(group, np.int64)
 
 
-def friend_pairs(x, link_len, periodic=True):
-    """All friend pairs (i < j) by the exact integer test; candidates from a k-d tree."""
+def friend_pairs(x, link_len, periodic=True, across_boundary=True):
+    """All friend pairs (i < j) by the exact integer test; candidates from a k-d tree.
+    across_boundary=False drops the pairs that are friends only through the
+    periodic wrap, which the reference's search never pairs: tree::find_groups
+    (src/tree.cpp:661-662, 701-702) rejects a node, and pairs a leaf, only
+    where the boxes intersect without the wrap (ranges_intersect), although
+    part_vect_find_groups measures the pair itself with the int32 wrap."""
     from scipy.spatial import cKDTree
     x = np.asarray(x, np.int32)
     n = len(x)
@@ -83,15 +88,19 @@ def friend_pairs(x, link_len, periodic=True):
     if len(pairs) == 0:
         return pairs.reshape(0, 2)
     d2 = _d2(x[pairs[:, 0]], x[pairs[:, 1]], periodic)
-    return pairs[(d2 < L2) & (d2 != 0)]
+    keep = (d2 < L2) & (d2 != 0)
+    if periodic and not across_boundary:
+        keep &= _d2(x[pairs[:, 0]], x[pairs[:, 1]], False) == d2
+    return pairs[keep]
 
 
-def groups(x, link_len, periodic=True):
-    """Group id per particle (smallest index in its group) or -1."""
+def groups(x, link_len, periodic=True, across_boundary=True):
+    """Group id per particle (smallest index in its group) or -1
+    (across_boundary: see friend_pairs)."""
     from scipy.sparse import coo_matrix
     from scipy.sparse.csgraph import connected_components
     n = len(x)
-    p = friend_pairs(x, link_len, periodic)
+    p = friend_pairs(x, link_len, periodic, across_boundary)
     out = np.full(n, DEFAULT, np.int64)
     if len(p) == 0:
         return out

@@ -27,6 +27,7 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 options options::global;
@@ -37,12 +38,9 @@ void options::set(options o) { global = o; }
 static std::vector<particle> g_init;
 part_vect initial_particle_set(std::string, int, int) { return g_init; }
 
-/* sky maps and groups are off (opts.map, opts.groups): src/map.cpp and
- * src/groups.cpp (Silo, HEALPix) are not built, and these are never reached */
+/* sky maps are off (opts.map): src/map.cpp (HEALPix, Silo) is not built,
+ * and this is never reached */
 void map_add_particle(const vect<double> &, double, double) { std::abort(); }
-void groups_add_finder(std::function<bool(void)>) { std::abort(); }
-void groups_add_particle1(particle) { std::abort(); }
-void groups_add_particle2(particle) { std::abort(); }
 
 /*
  * The reference's interaction lists as its walk hands them to the kernels:
@@ -296,6 +294,85 @@ extern "C" int reftree_kick(const int32_t *x, const float *v, const int8_t *rung
         for (int d = 0; d < 3; d++) v_out[3 * i + d] = ps[(size_t)i].v[d];
         rung_out[i] = (int8_t)ps[(size_t)i].flags.rung;
     }
+    return 0;
+}
+
+/*
+ * The reference's friends-of-friends partition (src/main.cpp:36-47 in
+ * solve_gravity): a tree refined as for a solve, compute_multipoles, then
+ * groups_reset, part_vect_init_groups, tree::find_groups from the root at
+ * theta 0.99 and groups_execute_finders until nothing changes.  label[i] is
+ * the reference's group id of caller particle i (its smallest storage index
+ * in the tree's order), -1 without friends.  Positions must be distinct.
+ * part_vect_find_groups caches the linking length on first use: one
+ * parameter set per library copy.
+ */
+extern "C" int reftree_fof(const int32_t *x, int64_t n, double link_len, int leaf_max, int64_t *label) {
+    options o = options();
+    o.problem = "caller";
+    o.problem_size = (std::uint64_t)n;
+    o.out_parts = (int)n;
+    o.m_tot = 1.0;
+    o.G = 1.0;
+    o.theta = 0.7;
+    o.parts_per_node = leaf_max;
+    o.link_len = link_len;
+    o.soft_len = 0.02;
+    o.t_max = 1.0;
+    o.dt_max = 1.0 / 64.0;
+    o.eta = 0.2;
+    o.ewald = true;
+    o.groups = true;
+    o.cosmic = false;
+    o.glass = false;
+    o.map = false;
+    o.workgroup_size = 32;
+    o.oversubscription = 1;
+    options::set(o);
+    g_init.assign((size_t)n, particle());
+    std::unordered_map<std::uint64_t, int64_t> index;
+    auto key = [](const int32_t *p) {
+        std::uint64_t h = 1469598103934665603ull;
+        for (int d = 0; d < 3; d++) h = (h ^ (std::uint32_t)p[d]) * 1099511628211ull;
+        return h;
+    };
+    for (int64_t i = 0; i < n; i++) {
+        particle &p = g_init[(size_t)i];
+        for (int d = 0; d < 3; d++) {
+            p.x[d] = x[3 * i + d];
+            p.v[d] = 0.0f;
+        }
+        p.flags.out = 1;
+        p.flags.rung = 0;
+        p.flags.group = DEFAULT_GROUP;
+        if (!index.emplace(key(x + 3 * i), i).second) return -2; /* positions (hashes) must be distinct */
+    }
+    cosmo_init(1.0, 0.0);
+    part_vect_init();
+    tree::set_theta(0.7);
+    tree_client root = hpx::new_<tree>(hpx::find_here(), 1, 0, (part_iter)n, 0).get();
+    refine_return rr;
+    do {
+        rr = root.refine(0);
+    } while (rr.rc);
+    root.compute_multipoles(0, false, 0);
+    auto root_list = std::vector<check_item>(1, root.get_check_item());
+    groups_reset();
+    part_vect_init_groups();
+    tree::set_theta(0.99);
+    root.find_groups(root_list, 0);
+    int rounds = 0;
+    while (groups_execute_finders())
+        if (++rounds > 100000) return -3;
+    const std::vector<particle> ps = part_vect_read(0, (part_iter)n).get();
+    for (const particle &p : ps) {
+        const int32_t q[3] = {p.x[0], p.x[1], p.x[2]};
+        const auto it = index.find(key(q));
+        if (it == index.end()) return -4;
+        label[it->second] = p.flags.group == DEFAULT_GROUP ? -1 : (int64_t)p.flags.group;
+    }
+    groups_reset();
+    hpx::release_components();
     return 0;
 }
 

@@ -65,6 +65,8 @@ def _lib(key):
             [C.c_void_p] * 3
         L.reftree_drift.restype = C.c_int
         L.reftree_drift.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.reftree_fof.restype = C.c_int
+        L.reftree_fof.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_void_p]
         L.reftree_cosmo_steps.restype = C.c_int
         L.reftree_cosmo_steps.argtypes = [C.c_double] * 5 + [C.c_void_p, C.c_int, C.c_void_p]
         _libs[key] = L
@@ -168,3 +170,18 @@ def drift(x, v, mrung):
     if rc != 0:
         raise RuntimeError("reftree_drift: %d" % rc)
     return xo
+
+
+def fof(x, link_len, leaf_max=64):
+    """The reference's friends-of-friends partition (tree::find_groups and
+    part_vect_find_groups driven as solve_gravity drives them): per caller
+    particle its group id (the reference's smallest storage index in the
+    group), -1 without friends."""
+    x = np.ascontiguousarray(x, np.int32)
+    n = len(x)
+    label = np.zeros(n, np.int64)
+    rc = _lib(("fof", n, float(link_len), int(leaf_max))).reftree_fof(x.ctypes.data, n, float(link_len),
+                                                                      int(leaf_max), label.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_fof: %d" % rc)
+    return label

@@ -192,3 +192,68 @@ def test_fof_catalog_64cubed_matches_oracle():
     assert np.allclose(c["dv"], ref["dv"], rtol=1e-5, atol=1e-6)
     assert np.allclose(c["rmax"], ref["rmax"], rtol=1e-5, atol=1e-9)
     assert np.allclose(c["rc"], ref["rc"], rtol=1e-5, atol=1e-9)
+
+
+# ---- the partition against the reference's own find_groups -----------------
+# (src/tree.cpp + src/part_vect.cpp + src/groups.cpp compiled into
+# oracle/_ref/libtg_reftree.so; skipped where it was not built)
+
+def _canon(label):
+    """group id = the smallest caller index in the group, -1 alone"""
+    out = np.full(len(label), -1, np.int64)
+    for g in np.unique(label[label >= 0]):
+        m = np.nonzero(label == g)[0]
+        out[m] = m.min()
+    return out
+
+
+def _distinct_planted(n, seed):
+    """uniform particles, four clumps of 40 inside the box and a chain of
+    three through the x = +-1/2 face; all positions distinct"""
+    rng = np.random.default_rng(seed)
+    x = rng.integers(-2 ** 31, 2 ** 31, size=(n, 3), dtype=np.int64)
+    L, _ = ofof.link_int(n, 0.2)
+    x[6] = [2 ** 31 - L // 3, 0, 0]
+    x[7] = [-2 ** 31 + L // 3, 0, 0]
+    x[8] = [-2 ** 31 + L, 0, 0]
+    for c in range(4):
+        base = np.array([-2 ** 30 + c * 2 ** 29, c * 2 ** 28, -c * 2 ** 28])
+        k = slice(16 + 40 * c, 16 + 40 * (c + 1))
+        x[k] = base + rng.integers(-L // 2, L // 2, size=(40, 3))
+    x = ((x + 2 ** 31) % 2 ** 32 - 2 ** 31).astype(np.int32)
+    assert len(np.unique(x, axis=0)) == n
+    return x
+
+
+@pytest.mark.parametrize("case", ["planted400", "planted3000", "uniform4096_l03", "uniform4096_l04_leaf16"])
+def test_partition_matches_reference_find_groups(case):
+    """The reference's own group finder (tree::find_groups at theta 0.99 and
+    part_vect_find_groups until nothing changes) gives the oracle's partition
+    without the friends that only the periodic wrap makes: the reference's
+    tree search tests box intersection without the wrap, so it never pairs
+    particles across the box boundary.  The CUDA path and the oracle keep
+    those links (the partition of the periodic friend relation); the two
+    partitions differ exactly there."""
+    import ref_tree
+    if not ref_tree.available():
+        pytest.skip("oracle/_ref/libtg_reftree.so not built")
+    from tigergrav_b200 import ics
+    leaf = 64
+    if case.startswith("planted"):
+        x, ll = _distinct_planted(int(case[7:]), 3), 0.2
+    else:
+        x, ll = ics.uniform(4096, 1), 0.3 if "l03" in case else 0.4
+        leaf = 16 if "leaf16" in case else 64
+    ref = _canon(ref_tree.fof(x, ll, leaf))
+    np.testing.assert_array_equal(ref, _canon(ofof.groups(x, ll, True, across_boundary=False)))
+    full = _canon(ofof.groups(x, ll, True))
+    diff = np.nonzero(full != ref)[0]
+    if len(diff):  # only groups that a boundary-crossing link joins or creates
+        wrap = ofof.friend_pairs(x, ll, True)
+        wrap = wrap[ofof._d2(x[wrap[:, 0]], x[wrap[:, 1]], False) != ofof._d2(x[wrap[:, 0]], x[wrap[:, 1]], True)]
+        touched = set(full[np.unique(wrap)])
+        assert set(full[diff]) <= touched
+    if case.startswith("planted"):
+        # the chain through the face: one group here, 7-8 and a lone 6 in the reference
+        assert full[6] == full[7] == full[8] >= 0
+        assert ref[6] == -1 and ref[7] == ref[8] >= 0
