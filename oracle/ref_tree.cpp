@@ -307,7 +307,20 @@ extern "C" int reftree_kick(const int32_t *x, const float *v, const int8_t *rung
  * part_vect_find_groups caches the linking length on first use: one
  * parameter set per library copy.
  */
+extern std::unordered_map<std::uint64_t, group> map[1024]; /* groups.cpp's catalogue, NMAP buckets */
+extern "C" int reftree_fof_catalog(const int32_t *x, const float *v, int64_t n, double link_len, int leaf_max,
+                                   int64_t *label, int64_t cap, double *cat, int64_t *ngroups);
 extern "C" int reftree_fof(const int32_t *x, int64_t n, double link_len, int leaf_max, int64_t *label) {
+    return reftree_fof_catalog(x, nullptr, n, link_len, leaf_max, label, 0, nullptr, nullptr);
+}
+
+/* the groups' catalogue of groups.cpp (the kick's groups_add_particle1 for
+ * every grouped particle, groups_finish1, part_vect_find_groups2,
+ * groups_finish2; src/main.cpp:56-66), after the partition above: per group
+ * (up to cap) 13 doubles in cat -- its id, N, centre (3), v (3), dv (3),
+ * rmax, rc; *ngroups = their number (velocities from v, which may be NULL) */
+extern "C" int reftree_fof_catalog(const int32_t *x, const float *v, int64_t n, double link_len, int leaf_max,
+                                   int64_t *label, int64_t cap, double *cat, int64_t *ngroups) {
     options o = options();
     o.problem = "caller";
     o.problem_size = (std::uint64_t)n;
@@ -340,7 +353,7 @@ extern "C" int reftree_fof(const int32_t *x, int64_t n, double link_len, int lea
         particle &p = g_init[(size_t)i];
         for (int d = 0; d < 3; d++) {
             p.x[d] = x[3 * i + d];
-            p.v[d] = 0.0f;
+            p.v[d] = v ? v[3 * i + d] : 0.0f;
         }
         p.flags.out = 1;
         p.flags.rung = 0;
@@ -370,6 +383,39 @@ extern "C" int reftree_fof(const int32_t *x, int64_t n, double link_len, int lea
         const auto it = index.find(key(q));
         if (it == index.end()) return -4;
         label[it->second] = p.flags.group == DEFAULT_GROUP ? -1 : (int64_t)p.flags.group;
+    }
+    if (cat) {
+        /* the output kick (zero forces: velocities stay) feeds groups_add_particle1 */
+        std::vector<force> f((size_t)n);
+        for (auto &q : f) {
+            q.phi = 0.0f;
+            q.g = vect<float>(0.0f);
+        }
+        kick_rc.out.clear();
+        part_vect_kick(0, (part_iter)n, 0, true, std::move(f)).get();
+        kick_rc.out.clear();
+        groups_finish1();
+        part_vect_find_groups2();
+        groups_finish2();
+        int64_t k = 0;
+        for (int m = 0; m < 1024; m++)
+            for (const auto &entry : map[m]) {
+                if (k < cap) {
+                    double *o = cat + 13 * k;
+                    const group &gr = entry.second;
+                    o[0] = (double)entry.first;
+                    o[1] = (double)gr.N;
+                    for (int d = 0; d < 3; d++) {
+                        o[2 + d] = gr.x[d];
+                        o[5 + d] = gr.v[d];
+                        o[8 + d] = gr.dv[d];
+                    }
+                    o[11] = gr.rmax;
+                    o[12] = gr.rc;
+                }
+                k++;
+            }
+        *ngroups = k;
     }
     groups_reset();
     hpx::release_components();

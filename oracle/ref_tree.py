@@ -65,6 +65,9 @@ def _lib(key):
             [C.c_void_p] * 3
         L.reftree_drift.restype = C.c_int
         L.reftree_drift.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.reftree_fof_catalog.restype = C.c_int
+        L.reftree_fof_catalog.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_void_p,
+                                          C.c_int64, C.c_void_p, C.c_void_p]
         L.reftree_fof.restype = C.c_int
         L.reftree_fof.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_void_p]
         L.reftree_cosmo_steps.restype = C.c_int
@@ -185,3 +188,23 @@ def fof(x, link_len, leaf_max=64):
     if rc != 0:
         raise RuntimeError("reftree_fof: %d" % rc)
     return label
+
+
+def fof_catalog(x, v, link_len, leaf_max=64, cap=1 << 16):
+    """The partition of fof() and the reference's catalogue of it (groups.cpp
+    fed by the output kick, a = 1): (label, dict of arrays id (the
+    reference's group id), N, x, v, dv, rmax, rc)."""
+    x = np.ascontiguousarray(x, np.int32)
+    v = np.ascontiguousarray(v, np.float32)
+    n = len(x)
+    label = np.zeros(n, np.int64)
+    cat = np.zeros((cap, 13))
+    ng = np.zeros(1, np.int64)
+    rc = _lib(("fofcat", n, float(link_len), int(leaf_max))).reftree_fof_catalog(
+        x.ctypes.data, v.ctypes.data, n, float(link_len), int(leaf_max), label.ctypes.data, cap, cat.ctypes.data,
+        ng.ctypes.data)
+    if rc != 0 or ng[0] > cap:
+        raise RuntimeError("reftree_fof_catalog: %d (%d groups)" % (rc, ng[0]))
+    c = cat[:ng[0]]
+    return label, dict(id=c[:, 0].astype(np.int64), N=c[:, 1].astype(np.int64), x=c[:, 2:5], v=c[:, 5:8],
+                       dv=c[:, 8:11], rmax=c[:, 11], rc=c[:, 12])

@@ -257,3 +257,31 @@ def test_partition_matches_reference_find_groups(case):
         # the chain through the face: one group here, 7-8 and a lone 6 in the reference
         assert full[6] == full[7] == full[8] >= 0
         assert ref[6] == -1 and ref[7] == ref[8] >= 0
+
+
+def test_catalog_matches_reference_groups():
+    """The oracle's catalogue against groups.cpp itself (fed by the
+    reference's output kick), on the reference's partition: the same groups
+    and sizes, centres and radii equal, mean velocity and dispersion within the
+    rounding of the reference's float sums (the oracle sums in double)."""
+    import ref_tree
+    if not ref_tree.available():
+        pytest.skip("oracle/_ref/libtg_reftree.so not built")
+    x = _distinct_planted(3000, 3)
+    v = (np.random.default_rng(2).standard_normal((3000, 3)) * 0.1).astype(np.float32)
+    label, cat = ref_tree.fof_catalog(x, v, 0.2)
+    first = {}
+    for i, g in enumerate(label):
+        if g >= 0:
+            first.setdefault(g, i)
+    gid = np.array([first[g] for g in cat["id"]])
+    order = np.argsort(gid)
+    mine = ofof.catalog(x, v, _canon(ofof.groups(x, 0.2, True, across_boundary=False)), a=1.0)
+    np.testing.assert_array_equal(gid[order], mine["id"])
+    assert len(gid) >= 40
+    np.testing.assert_array_equal(cat["N"][order], mine["N"])
+    np.testing.assert_allclose(cat["x"][order], mine["x"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(cat["rmax"][order], mine["rmax"], rtol=1e-6)
+    np.testing.assert_allclose(cat["rc"][order], mine["rc"], rtol=1e-6)
+    np.testing.assert_allclose(cat["v"][order], mine["v"], rtol=0, atol=1e-7)
+    np.testing.assert_allclose(cat["dv"][order], mine["dv"], rtol=0, atol=1e-7)
