@@ -20,6 +20,7 @@
 #include <tigergrav/cosmo.hpp>
 #include <tigergrav/gravity.hpp>
 #include <tigergrav/groups.hpp>
+#include <tigergrav/load.hpp>
 #include <tigergrav/map.hpp>
 #include <tigergrav/options.hpp>
 #include <tigergrav/part_vect.hpp>
@@ -419,6 +420,25 @@ extern "C" int reftree_fof_catalog(const int32_t *x, const float *v, int64_t n, 
     }
     groups_reset();
     hpx::release_components();
+    return 0;
+}
+
+/* The reference's Gadget-1 reader (src/load.cpp:34-96, compiled into this
+ * library with src/rand.cpp for its output flag): up to cap particles' int32
+ * positions and float velocities of the file, *n their number. */
+extern "C" int reftree_load_gadget1(const char *path, int64_t cap, int32_t *x, float *v, int64_t *n) {
+    options o = options::get();
+    o.out_parts = 0;
+    o.problem_size = 1;
+    options::set(o);
+    const std::vector<particle> ps = load_particles(std::string(path));
+    *n = (int64_t)ps.size();
+    if (*n > cap) return -1;
+    for (int64_t i = 0; i < *n; i++)
+        for (int d = 0; d < 3; d++) {
+            x[3 * i + d] = ps[(size_t)i].x[d];
+            v[3 * i + d] = ps[(size_t)i].v[d];
+        }
     return 0;
 }
 

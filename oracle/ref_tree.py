@@ -65,6 +65,8 @@ def _lib(key):
             [C.c_void_p] * 3
         L.reftree_drift.restype = C.c_int
         L.reftree_drift.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.reftree_load_gadget1.restype = C.c_int
+        L.reftree_load_gadget1.argtypes = [C.c_char_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         L.reftree_fof_catalog.restype = C.c_int
         L.reftree_fof_catalog.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_void_p,
                                           C.c_int64, C.c_void_p, C.c_void_p]
@@ -208,3 +210,15 @@ def fof_catalog(x, v, link_len, leaf_max=64, cap=1 << 16):
     c = cat[:ng[0]]
     return label, dict(id=c[:, 0].astype(np.int64), N=c[:, 1].astype(np.int64), x=c[:, 2:5], v=c[:, 5:8],
                        dv=c[:, 8:11], rmax=c[:, 11], rc=c[:, 12])
+
+
+def load_gadget1(path, cap=1 << 22):
+    """The reference's load_particles (src/load.cpp:34-96): int32 positions
+    and float velocities of a Gadget-1 file."""
+    x = np.zeros((cap, 3), np.int32)
+    v = np.zeros((cap, 3), np.float32)
+    n = np.zeros(1, np.int64)
+    rc = _lib(("load",)).reftree_load_gadget1(str(path).encode(), cap, x.ctypes.data, v.ctypes.data, n.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reftree_load_gadget1: %d" % rc)
+    return x[:n[0]].copy(), v[:n[0]].copy()
