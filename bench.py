@@ -111,7 +111,7 @@ LEAF_FLOPS = {"PC_D": 581, "PC_E": 7800, "PP_E": 1460}
 # theta 0.19, leaf 48 (the clustered72 workload); k_ewald_chunk on the 128^3
 # clustered box at theta 0.3.  Scaled by this run's counts on the assumption
 # that traffic grows with the interactions.
-TRAFFIC = {"pp": {"PP_D": 4.7e-3}, "nodes": {"CC_E": 2.65, "CP_E": 2.65}, "leaf": {"PP_E": 1.56, "PC_E": 1.56}}
+TRAFFIC = {"pp": {"PP_D": 4.6e-3}, "nodes": {"CC_E": 2.65, "CP_E": 2.65}, "leaf": {"PP_E": 1.61, "PC_E": 1.61}}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per interaction of a small capture, "
                   "scaled by this run's interaction counts")
 
