@@ -217,3 +217,24 @@ def test_gpu_walk_matches_reference_walk(name, oracle_mod):
         ref, mine = _canonical(x, s, r["calls"])
     assert len(ref) == len(mine)
     assert ref == mine
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["clustered16_free_t07", "clustered12_ewald_t07_leaf24"])
+def test_gpu_forces_match_reference_solve(name, oracle_mod):
+    """the CUDA path's FP32 forces against the reference's own whole solve
+    (its tree, walk and kernels), per particle: no further from the FP64
+    evaluation of the same lists than the reference's run is, plus 1e-5 of
+    the force (the bound of tests/helpers.py)"""
+    import tigergrav_b200 as tg
+    from helpers import arbiter_excess
+    x, r, o = _case(name, oracle_mod)
+    c = CASES[name]
+    with tg.GravitySolver(len(x), theta=c["theta"], ewald=c["ewald"], leaf_max=c["leaf"]) as s:
+        s.set_particles(x).solve_gravity()
+        phi, g = s.get_forces()
+    o.evaluate(fp64=True)
+    phi64, g64 = o.forces()
+    fx, px = arbiter_excess(g, r["g"].astype(np.float64), g64, phi, r["phi"].astype(np.float64), phi64)
+    assert fx <= 0.0, fx
+    assert px <= 0.0, px
