@@ -46,7 +46,10 @@ times that kind's host throughput, sampled by running the reference kernel
 over random sinks of this workload with their real lists.  The reference arm
 also times full evaluations with the reference kernels on all host cores
 where one fits in seconds: the 32^3 uniform box and the 128^3 clustered box,
-both at theta 0.7 (``measured_full``).
+both at theta 0.7 (``measured_full``), and the 32^3 box once more with the
+reference's own tree, walk and kernels (src/tree.cpp, part_vect.cpp,
+gravity.cpp compiled into oracle/_ref) run serially on one core, its
+interaction counts checked against the restated walk's.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
   torchrun --nproc-per-node N bench.py --gpus N ...   (independent replicas)
@@ -249,6 +252,28 @@ def cpu_full_eval(x, theta, nthreads):
             "kind": "reference" if use_ref else "port", "cores": nthreads}
 
 
+def reference_code_eval(x, theta):
+    """One full evaluation by the reference's own code -- src/tree.cpp's
+    refine, compute_multipoles and kick_fmm, src/part_vect.cpp and its
+    kernels -- compiled where it lies into oracle/_ref/libtg_reftree.so and
+    run serially on one core through a single-locality HPX stand-in (the
+    reference runs it on HPX threads).  None when that library was not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_tree
+    if not ref_tree.available():
+        return None
+    t0 = time.perf_counter()
+    r = ref_tree.solve(x, theta, True, 64)
+    sec = time.perf_counter() - t0
+    O = _oracle()
+    o = O.Oracle(theta=theta, ewald=True, leaf_max=64).set_particles(x)
+    o.build().multipoles().walk(nthreads=os.cpu_count() or 1)
+    same = o.stats()[0] == r["stats"]
+    return {"seconds": sec, "mparticles_per_s": len(x) / sec / 1e6, "theta": theta, "n": int(len(x)), "cores": 1,
+            "kind": "reference code (serial)", "interaction_stats": r["stats"],
+            "stats_equal_restated_walk": bool(same)}
+
+
 def reference_arm(args, w, cfg):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -271,6 +296,9 @@ def reference_arm(args, w, cfg):
     cb["value"] = v
     full = {"uniform32_theta0.7": cpu_full_eval(ics.uniform(32768, 1), 0.7, nth),
             "clustered128_theta0.7": cpu_full_eval(ics.clustered(128, 2), 0.7, nth)}
+    own = reference_code_eval(ics.uniform(32768, 1), 0.7)
+    if own is not None:
+        full["uniform32_theta0.7_reference_code"] = own
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mparticles/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 sums)", "data": "synthetic (seeded)",
